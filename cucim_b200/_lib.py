@@ -1,0 +1,126 @@
+"""ctypes binding of libcimx.so (the C ABI declared in include/cimx.h).
+
+The shared library is built in-tree by ``cucim_b200/build.py``. There is no
+fallback: if the library is missing, importing this module raises.
+"""
+
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libcimx.so")
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError(
+        f"libcimx.so not found at {LIB_PATH}; build it with "
+        "`python -m cucim_b200.build` (nvcc, sm_100a)"
+    )
+
+lib = ctypes.CDLL(LIB_PATH)
+
+MAX_NDIM = 8
+
+MODE_CODES = {
+    "reflect": 0,
+    "grid-mirror": 0,
+    "mirror": 1,
+    "nearest": 2,
+    "grid-wrap": 3,
+    "wrap": 3,
+    "constant": 4,
+}
+
+F_W64 = 1 << 0
+F_CONVOLVE = 1 << 1
+F_CVAL_AS_INPUT = 1 << 2
+F_SKIP_ZERO_TAPS = 1 << 3
+L_NO_FUSION = 1 << 0
+
+E_INVALID, E_DTYPE, E_CUDA, E_NOMEM, E_LAYOUT, E_TIMEOUT = -1, -2, -3, -4, -5, -6
+
+
+class CimxArray(ctypes.Structure):
+    _fields_ = [
+        ("data", ctypes.c_void_p),
+        ("dtype", ctypes.c_int32),
+        ("ndim", ctypes.c_int32),
+        ("shape", ctypes.c_int64 * MAX_NDIM),
+        ("strides", ctypes.c_int64 * MAX_NDIM),
+    ]
+
+
+class CimxPass(ctypes.Structure):
+    _fields_ = [
+        ("axis", ctypes.c_int32),
+        ("ntaps", ctypes.c_int32),
+        ("origin", ctypes.c_int32),
+        ("mode", ctypes.c_int32),
+        ("cval", ctypes.c_double),
+        ("flags", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+        ("taps", ctypes.POINTER(ctypes.c_double)),
+    ]
+
+
+_P = ctypes.POINTER
+_A = _P(CimxArray)
+_sigs = {
+    "cimx_abi_version": ([], ctypes.c_int),
+    "cimx_last_error_string": ([], ctypes.c_char_p),
+    "cimx_set_allocator": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
+    "cimx_correlate1d": (
+        [_A, _A, _P(ctypes.c_double), ctypes.c_int, ctypes.c_int, ctypes.c_int,
+         ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_void_p],
+        ctypes.c_int,
+    ),
+    "cimx_separable": (
+        [_A, _A, _P(CimxPass), ctypes.c_int, ctypes.c_int, ctypes.c_void_p], ctypes.c_int,
+    ),
+    "cimx_gradient_magnitude": (
+        [_A, _A, _P(CimxPass), ctypes.c_int, ctypes.c_int, ctypes.c_void_p], ctypes.c_int,
+    ),
+    "cimx_eigvals_sym": (
+        [_A, ctypes.c_int, _A, ctypes.c_int, ctypes.c_int, ctypes.c_void_p], ctypes.c_int,
+    ),
+    "cimx_rgb2gray": ([_A, _A, ctypes.c_void_p], ctypes.c_int),
+    "cimx_convert": ([_A, _A, ctypes.c_int, ctypes.c_void_p], ctypes.c_int),
+    "cimx_gradient_fd": ([_A, _A, ctypes.c_int, ctypes.c_void_p], ctypes.c_int),
+    "cimx_frangi_accumulate": (
+        [_A, ctypes.c_int, _A, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+         ctypes.c_void_p, ctypes.c_void_p],
+        ctypes.c_int,
+    ),
+}
+for _name, (_args, _res) in _sigs.items():
+    _fn = getattr(lib, _name)
+    _fn.argtypes = _args
+    _fn.restype = _res
+
+EXPORTED = tuple(_sigs)
+
+
+def last_error():
+    msg = lib.cimx_last_error_string()
+    return msg.decode() if msg else ""
+
+
+def check(rc, what):
+    """Raise the exception cuCIM raises for the condition behind `rc`."""
+    if rc == 0:
+        return
+    msg = last_error() or what
+    if rc == E_NOMEM:
+        raise MemoryError(msg)
+    if rc == E_DTYPE:
+        raise TypeError(msg)
+    if rc == E_INVALID and "origin" in msg:
+        raise ValueError(msg)
+    raise RuntimeError(f"{what}: {msg}")
+
+
+def taps_pointer(taps):
+    """A float64 C-contiguous copy of `taps` and a pointer into it."""
+    t = np.ascontiguousarray(np.asarray(taps, dtype=np.float64))
+    return t, t.ctypes.data_as(_P(ctypes.c_double))

@@ -1,0 +1,53 @@
+// cimx_internal.h — host-side interfaces between the C-ABI layer and the
+// kernel families of libcimx.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/cimx.h"
+
+namespace cimx {
+
+// Taps travel to the kernels inside the launch parameters (no host->device
+// copy per call) up to this many bytes; longer tap vectors are copied into
+// scratch memory.
+constexpr int kParamTapBytes = 4096;
+
+// A single 1-D pass over the C-contiguous view (outer, L, inner) of the
+// input, along the middle axis.
+struct PassDesc {
+  const void* in;
+  void* out;
+  int tin, tout;
+  int64_t outer, L, inner;
+  int axis;        // axis of the array the pass runs along
+  int K;           // taps
+  int anchor;      // tap k reads input coordinate l - anchor + k
+  int mode;        // CIMX_MODE_*
+  double cval;     // caller's fill value
+  bool w64;        // weights type is float64
+  bool cval_as_input;
+  bool skip_zero;  // skip zero taps (only matters for non-finite inputs)
+  const double* taps;  // host taps, already flipped for convolution, not yet rounded
+};
+
+void set_error(const std::string& msg);
+int fail(int code, const std::string& msg);
+int cuda_fail(cudaError_t e, const char* what);
+
+// scratch memory through the installed allocator
+void* scratch_alloc(size_t nbytes, cudaStream_t s);
+void scratch_free(void* p, size_t nbytes, cudaStream_t s);
+
+// generic single pass (cimx_pass.cu)
+int launch_generic_pass(const PassDesc& d, cudaStream_t stream);
+
+// elementwise helpers (cimx_elementwise.cu)
+int launch_square_accumulate(void* acc, const void* term, int dt, int64_t n, bool first,
+                             cudaStream_t stream);
+int launch_sqrt_inplace(void* acc, int dt, int64_t n, cudaStream_t stream);
+
+}  // namespace cimx

@@ -1,0 +1,289 @@
+// cimx_pass.cu — the generic single-pass separable correlation kernels.
+//
+// One launch applies one 1-D correlation along the middle axis of the
+// C-contiguous view (outer, L, inner) of an n-D array: any axis, any real
+// dtype pair, any tap count, every boundary mode. These kernels serve every
+// call the fused kernels (cimx_fused.cu) do not take.
+//
+// Per output the arithmetic is cuCIM's: taps in ascending order, one fused
+// multiply-add chain in W starting from +0, then cast<D>() (see
+// cimx_common.cuh). The halo'd tile is staged in shared memory once, each
+// thread keeps a sliding window of 2*P inputs in registers and produces P
+// consecutive outputs, so a tap costs one broadcast shared load per P FMAs.
+#include <algorithm>
+#include <mutex>
+#include <vector>
+
+#include "cimx_common.cuh"
+#include "cimx_internal.h"
+
+namespace cimx {
+namespace {
+
+constexpr int P = 8;            // outputs per thread along the filtered axis
+constexpr int kColTI = 32;      // column kernel: inner-axis width of a tile
+constexpr int kColTY = 8;       // column kernel: threads along the filtered axis
+constexpr int kColTL = kColTY * P;
+constexpr int kMaxSmem = 227 * 1024;
+
+template <class W>
+struct TapBlock {
+  W w[kParamTapBytes / sizeof(W)];
+};
+
+struct GArgs {
+  const void* in;
+  void* out;
+  int tin, tout;
+  long long outer, L, inner;
+  int K, K8, anchor, mode;
+  double cval;
+  int cval_as_input;
+  const void* gtaps;   // device copy of the taps when they exceed the parameter block
+  long long tiles_a, tiles_b;
+};
+
+template <class W>
+__device__ __forceinline__ void load_taps(W* taps, const GArgs& a, const TapBlock<W>& tb,
+                                          int tid, int nthr) {
+  const W* src = a.gtaps ? static_cast<const W*>(a.gtaps) : tb.w;
+  for (int k = tid; k < a.K8; k += nthr) taps[k] = k < a.K ? src[k] : W(0);
+}
+
+// Sliding-window tap loop shared by the row and column kernels. `at(q)`
+// returns the staged input at logical offset q from this thread's first
+// output; the chain for output p is acc[p] = fma(x[p + k], w[k], acc[p]).
+template <class W, bool SKIPZ, class At>
+__device__ __forceinline__ void tap_loop(W (&acc)[P], const W* taps, int K, At at) {
+  W win[2 * P];
+#pragma unroll
+  for (int j = 0; j < P; ++j) win[j] = at(j);
+  for (int k0 = 0; k0 < K; k0 += P) {
+#pragma unroll
+    for (int j = 0; j < P; ++j) win[P + j] = at(k0 + P + j);
+#pragma unroll
+    for (int j = 0; j < P; ++j) {
+      const W w = taps[k0 + j];
+      if (k0 + j < K && (!SKIPZ || w != W(0))) {
+#pragma unroll
+        for (int p = 0; p < P; ++p) acc[p] = fma(win[p + j], w, acc[p]);
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < P; ++j) win[j] = win[P + j];
+  }
+}
+
+// Filter along the contiguous last axis (inner == 1). Block = (seg_threads,
+// rows); each row buffer is padded by one word every 8 so that lanes reading
+// at a stride of P words hit distinct banks.
+template <class W, bool SKIPZ>
+__global__ void __launch_bounds__(256) k_rows(GArgs a, TapBlock<W> tb) {
+  extern __shared__ __align__(16) unsigned char sm_raw[];
+  W* taps = reinterpret_cast<W*>(sm_raw);
+  const int nthr = blockDim.x * blockDim.y;
+  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+  load_taps(taps, a, tb, tid, nthr);
+  const int seg = blockDim.x * P;
+  const int span = seg + a.K8 + P;
+  const int pspan = span + (span >> 3) + 1;
+  W* rb = taps + a.K8 + threadIdx.y * pspan;
+
+  const long long sg = blockIdx.x % a.tiles_b;
+  const long long rg = blockIdx.x / a.tiles_b;
+  const long long row = rg * blockDim.y + threadIdx.y;
+  const long long x0 = sg * seg;
+  const W cv = fill_value<W>(a.cval, a.cval_as_input, a.tin);
+  const long long rbase = row * a.L;
+  if (row < a.outer) {
+    for (int j = threadIdx.x; j < span; j += blockDim.x) {
+      const long long m = map_coord(x0 - a.anchor + j, a.L, a.mode);
+      rb[j + (j >> 3)] = m < 0 ? cv : load_as<W>(a.in, rbase + m, a.tin);
+    }
+  }
+  __syncthreads();
+  if (row >= a.outer) return;
+  const int b = threadIdx.x * P;
+  W acc[P];
+#pragma unroll
+  for (int p = 0; p < P; ++p) acc[p] = W(0);
+  tap_loop<W, SKIPZ>(acc, taps, a.K, [&](int q) {
+    const int x = b + q;
+    return rb[x + (x >> 3)];
+  });
+#pragma unroll
+  for (int p = 0; p < P; ++p) {
+    const long long x = x0 + b + p;
+    if (x < a.L) store_cast<W>(a.out, rbase + x, acc[p], a.tout);
+  }
+}
+
+// Filter along a strided axis (inner > 1). Block = (32 inner columns, 8);
+// each thread produces P consecutive outputs of one column.
+template <class W, bool SKIPZ>
+__global__ void __launch_bounds__(256) k_cols(GArgs a, TapBlock<W> tb) {
+  extern __shared__ __align__(16) unsigned char sm_raw[];
+  W* taps = reinterpret_cast<W*>(sm_raw);
+  const int tid = threadIdx.y * kColTI + threadIdx.x;
+  load_taps(taps, a, tb, tid, kColTI * kColTY);
+  W* buf = taps + a.K8;
+  const int span = kColTL + a.K8 + P;
+
+  long long bid = blockIdx.x;
+  const long long it = bid % a.tiles_a;
+  bid /= a.tiles_a;
+  const long long lt = bid % a.tiles_b;
+  const long long o = bid / a.tiles_b;
+  const long long i = it * kColTI + threadIdx.x;
+  const long long l0 = lt * kColTL;
+  const W cv = fill_value<W>(a.cval, a.cval_as_input, a.tin);
+  const long long obase = o * a.L;
+  for (int j = threadIdx.y; j < span; j += kColTY) {
+    W v = W(0);
+    if (i < a.inner) {
+      const long long m = map_coord(l0 - a.anchor + j, a.L, a.mode);
+      v = m < 0 ? cv : load_as<W>(a.in, (obase + m) * a.inner + i, a.tin);
+    }
+    buf[j * kColTI + threadIdx.x] = v;
+  }
+  __syncthreads();
+  if (i >= a.inner) return;
+  const int b = threadIdx.y * P;
+  W acc[P];
+#pragma unroll
+  for (int p = 0; p < P; ++p) acc[p] = W(0);
+  tap_loop<W, SKIPZ>(acc, taps, a.K, [&](int q) { return buf[(b + q) * kColTI + threadIdx.x]; });
+#pragma unroll
+  for (int p = 0; p < P; ++p) {
+    const long long l = l0 + b + p;
+    if (l < a.L) store_cast<W>(a.out, (obase + l) * a.inner + i, acc[p], a.tout);
+  }
+}
+
+// Tap counts whose halo does not fit in shared memory: one thread per
+// output, reading global memory per tap (taps in global memory).
+template <class W, bool SKIPZ>
+__global__ void __launch_bounds__(256) k_direct(GArgs a) {
+  const W* taps = static_cast<const W*>(a.gtaps);
+  const W cv = fill_value<W>(a.cval, a.cval_as_input, a.tin);
+  const long long total = a.outer * a.L * a.inner;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const long long i = e % a.inner;
+    const long long ol = e / a.inner;
+    const long long l = ol % a.L;
+    const long long obase = (ol - l);
+    W acc = W(0);
+    for (int k = 0; k < a.K; ++k) {
+      const W w = taps[k];
+      if (SKIPZ && w == W(0)) continue;
+      const long long m = map_coord(l - a.anchor + k, a.L, a.mode);
+      const W x = m < 0 ? cv : load_as<W>(a.in, (obase + m) * a.inner + i, a.tin);
+      acc = fma(x, w, acc);
+    }
+    store_cast<W>(a.out, e, acc, a.tout);
+  }
+}
+
+template <class Kern>
+void allow_big_smem(Kern k) {
+  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem);
+}
+
+template <class W, bool SKIPZ>
+int launch_t(GArgs a, const TapBlock<W>& tb, bool direct, cudaStream_t st) {
+  static std::once_flag once;
+  std::call_once(once, [] {
+    allow_big_smem(k_rows<W, SKIPZ>);
+    allow_big_smem(k_cols<W, SKIPZ>);
+  });
+  const long long total = a.outer * a.L * a.inner;
+  if (total == 0) return CIMX_OK;
+  if (direct) {
+    const long long blocks = std::min<long long>((total + 255) / 256, 148LL * 64);
+    k_direct<W, SKIPZ><<<(unsigned)blocks, 256, 0, st>>>(a);
+  } else if (a.inner == 1) {
+    int seg_threads = 256;
+    while (seg_threads > 32 && (long long)(seg_threads / 2) * P >= a.L) seg_threads /= 2;
+    const int ry = 256 / seg_threads;
+    const int seg = seg_threads * P;
+    const int span = seg + a.K8 + P;
+    const int pspan = span + (span >> 3) + 1;
+    const size_t smem = sizeof(W) * ((size_t)a.K8 + (size_t)ry * pspan);
+    a.tiles_b = (a.L + seg - 1) / seg;
+    const long long blocks = ((a.outer + ry - 1) / ry) * a.tiles_b;
+    k_rows<W, SKIPZ><<<(unsigned)blocks, dim3(seg_threads, ry), smem, st>>>(a, tb);
+  } else {
+    const size_t smem = sizeof(W) * ((size_t)a.K8 + (size_t)(kColTL + a.K8 + P) * kColTI);
+    a.tiles_a = (a.inner + kColTI - 1) / kColTI;
+    a.tiles_b = (a.L + kColTL - 1) / kColTL;
+    const long long blocks = a.tiles_a * a.tiles_b * a.outer;
+    k_cols<W, SKIPZ><<<(unsigned)blocks, dim3(kColTI, kColTY), smem, st>>>(a, tb);
+  }
+  return cuda_fail(cudaGetLastError(), "generic pass launch");
+}
+
+template <class W>
+int launch_w(const PassDesc& d, cudaStream_t st) {
+  // Round the taps to W, then (elementwise-kernel rule) drop zero taps at
+  // both ends: skipping them is exact whatever the input holds.
+  std::vector<W> w(d.K);
+  for (int k = 0; k < d.K; ++k) w[k] = static_cast<W>(d.taps[k]);
+  int lo = 0, hi = d.K;
+  if (d.skip_zero) {
+    while (lo < hi && w[lo] == W(0)) ++lo;
+    while (hi > lo && w[hi - 1] == W(0)) --hi;
+  }
+  const int K = hi - lo;
+  bool interior_zero = false;
+  if (d.skip_zero)
+    for (int k = lo; k < hi; ++k) interior_zero |= (w[k] == W(0));
+
+  GArgs a{};
+  a.in = d.in;
+  a.out = d.out;
+  a.tin = d.tin;
+  a.tout = d.tout;
+  a.outer = d.outer;
+  a.L = d.L;
+  a.inner = d.inner;
+  a.K = K;
+  a.K8 = (K + P - 1) / P * P;
+  a.anchor = d.anchor - lo;
+  a.mode = d.mode;
+  a.cval = d.cval;
+  a.cval_as_input = d.cval_as_input ? 1 : 0;
+
+  TapBlock<W> tb;
+  std::fill(std::begin(tb.w), std::end(tb.w), W(0));
+  const bool fits_param = K * sizeof(W) <= sizeof(tb.w);
+  const size_t smem_rows = sizeof(W) * ((size_t)a.K8 + (size_t)(2048 + a.K8 + P) * 9 / 8 + 2);
+  const size_t smem_cols = sizeof(W) * ((size_t)a.K8 + (size_t)(kColTL + a.K8 + P) * kColTI);
+  const bool direct = (a.inner == 1 ? smem_rows : smem_cols) > (size_t)kMaxSmem;
+  void* gt = nullptr;
+  const size_t gbytes = sizeof(W) * std::max(K, 1);
+  if (fits_param && !direct) {
+    std::copy(w.begin() + lo, w.begin() + hi, tb.w);
+  } else {
+    gt = scratch_alloc(gbytes, st);
+    if (!gt) return fail(CIMX_E_NOMEM, "scratch allocation for taps failed");
+    cudaError_t e = cudaMemcpyAsync(gt, w.data() + lo, sizeof(W) * K, cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) {
+      scratch_free(gt, gbytes, st);
+      return cuda_fail(e, "tap upload");
+    }
+    a.gtaps = gt;
+  }
+  int rc = interior_zero ? launch_t<W, true>(a, tb, direct, st)
+                         : launch_t<W, false>(a, tb, direct, st);
+  if (gt) scratch_free(gt, gbytes, st);
+  return rc;
+}
+
+}  // namespace
+
+int launch_generic_pass(const PassDesc& d, cudaStream_t stream) {
+  return d.w64 ? launch_w<double>(d, stream) : launch_w<float>(d, stream);
+}
+
+}  // namespace cimx

@@ -1,0 +1,364 @@
+"""Drop-in for cuCIM's vendored ndimage separable filters.
+
+Same names, signatures, defaults, dtype rules and errors as
+cucim.skimage._vendored.ndimage (python/cucim/src/cucim/skimage/_vendored/
+_ndimage_filters.py, cited as FLT below); every filter runs in libcimx's
+sm_100a kernels through the C ABI of include/cimx.h. Arrays may be torch
+CUDA tensors, CuPy arrays or any __cuda_array_interface__ / DLPack object;
+results come back as the input's array type.
+"""
+
+import ctypes
+import math
+import warnings
+
+import numpy as np
+import torch
+
+from . import _arrays, _lib, _util
+
+__all__ = [
+    "correlate1d", "convolve1d", "uniform_filter1d", "uniform_filter",
+    "gaussian_filter1d", "gaussian_filter", "prewitt", "sobel",
+    "generic_gradient_magnitude", "gaussian_gradient_magnitude",
+]
+
+
+class _PassList:
+    """A list of CimxPass structs plus the tap arrays they point into."""
+
+    def __init__(self):
+        self.keep = []
+        self.items = []
+
+    def add(self, axis, taps, origin, mode, cval, flags):
+        t, ptr = _lib.taps_pointer(taps)
+        self.keep.append(t)
+        p = _lib.CimxPass()
+        p.axis, p.ntaps, p.origin = axis, t.size, origin
+        p.mode, p.cval, p.flags, p.reserved = _lib.MODE_CODES[mode], float(cval), flags, 0
+        p.taps = ptr
+        self.items.append(p)
+
+    def array(self):
+        arr = (_lib.CimxPass * max(1, len(self.items)))(*self.items)
+        return arr
+
+    def __len__(self):
+        return len(self.items)
+
+
+def _check_cval(mode, cval, out_dtype):
+    """UTIL:27-32."""
+    if mode == "constant" and np.dtype(out_dtype).kind in "iu" and not np.isfinite(cval):
+        raise NotImplementedError(
+            "Non-finite cval is not supported for outputs with integer dtype."
+        )
+
+
+def _build_passes(in_dtype, out_dtype, ndim, specs, cval, algorithm):
+    """Resolve (axis, weights, mode, origin, convolve) specs into CimxPasses.
+
+    The first pass reads the input's dtype, later ones the output's (the
+    intermediates of _run_1d_filters, _vendored/_ndimage_filters_core.py:145).
+    """
+    pl = _PassList()
+    for i, (axis, w, mode, origin, convolve) in enumerate(specs):
+        w = np.asarray(w)
+        if w.ndim != 1 or w.size < 1:
+            raise RuntimeError("incorrect filter size")
+        if w.dtype.kind == "c":
+            raise NotImplementedError("complex weights are not supported")
+        K = w.size
+        axis = _util.normalize_axis(axis, ndim)
+        origin = _util.check_origin(origin, K)
+        mode = "grid-wrap" if mode == "wrap" else mode
+        _util.check_mode(mode)
+        pass_in = in_dtype if i == 0 else out_dtype
+        if mode == "constant":
+            _check_cval(mode, cval, out_dtype)
+        flags = _util.pass_flags(pass_in, ndim, axis, K, origin, mode, cval, w.dtype,
+                                 convolve, algorithm)
+        pl.add(axis, w, origin, mode, cval, flags)
+    return pl
+
+
+def _run(input, specs, output, cval, algorithm=None):
+    """Apply the pass list to `input` into `output` (FLT:363-396 semantics)."""
+    x = _arrays.as_tensor(input)
+    if x.dtype.is_complex:
+        raise NotImplementedError("complex arrays are not supported")
+    xc = x.contiguous()
+    slot = _arrays.output_slot(output, input, xc)
+    out_dt = slot.dtype
+    pl = _build_passes(_arrays.np_dtype(xc), out_dt, xc.dim(), specs, cval, algorithm)
+    arr = pl.array()
+    a_in = _arrays.to_cimx(xc)
+    a_out = _arrays.to_cimx(slot.work)
+    rc = _lib.lib.cimx_separable(ctypes.byref(a_in), ctypes.byref(a_out), arr, len(pl), 0,
+                                 _arrays.stream_of(xc))
+    _lib.check(rc, "separable filter")
+    return slot.result()
+
+
+# --------------------------------------------------------------- correlate1d
+
+def _correlate_or_convolve1d(input, weights, axis, output, mode, cval, origin,
+                             convolution, algorithm):
+    x = _arrays.as_tensor(input)
+    axis = _util.normalize_axis(axis, x.dim())
+    w = _weights_to_host(weights)
+    if algorithm not in (None, "shared_memory", "elementwise"):
+        raise ValueError("algorithm must be 'shared_memory', 'elementwise' or None")
+    if algorithm == "shared_memory" and mode == "constant" and (
+        not np.isfinite(cval) or (cval < 0 and _arrays.np_dtype(x).kind == "u")
+    ):
+        warnings.warn(
+            f"{cval=} and input.dtype={_arrays.np_dtype(x)} is unsupported for algorithm "
+            "'shared_memory', falling back to elementwise"
+        )
+    return _run(input, [(axis, w, mode, origin, convolution)], output, cval, algorithm)
+
+
+def _weights_to_host(weights):
+    if isinstance(weights, np.ndarray):
+        return weights
+    if isinstance(weights, torch.Tensor):
+        return weights.detach().cpu().numpy()
+    if hasattr(weights, "__cuda_array_interface__") or hasattr(weights, "__dlpack__"):
+        return _arrays.as_tensor(weights).cpu().numpy()
+    return np.asarray(weights)
+
+
+def correlate1d(input, weights, axis=-1, output=None, mode="reflect", cval=0.0, origin=0,
+                *, algorithm=None):
+    """One-dimensional correlation along `axis` (FLT:135-178)."""
+    return _correlate_or_convolve1d(input, weights, axis, output, mode, cval, origin, False,
+                                    algorithm)
+
+
+def convolve1d(input, weights, axis=-1, output=None, mode="reflect", cval=0.0, origin=0,
+               *, algorithm=None):
+    """One-dimensional convolution along `axis` (FLT:180-221)."""
+    return _correlate_or_convolve1d(input, weights, axis, output, mode, cval, origin, True,
+                                    algorithm)
+
+
+# -------------------------------------------------------------- uniform
+
+def uniform_filter1d(input, size, axis=-1, output=None, mode="reflect", cval=0.0, origin=0,
+                     *, algorithm=None):
+    """FLT:399-444."""
+    x = _arrays.as_tensor(input)
+    wdt = np.promote_types(_arrays.np_dtype(x), np.float32)
+    w = np.full(size, 1 / size, dtype=wdt)
+    return correlate1d(input, w, axis, output, mode, cval, origin, algorithm=algorithm)
+
+
+def uniform_filter(input, size=3, output=None, mode="reflect", cval=0.0, origin=0, axes=None,
+                   *, algorithm=None):
+    """FLT:447-521."""
+    x = _arrays.as_tensor(input)
+    axes = _util.check_axes(axes, x.dim())
+    n = len(axes)
+    sizes = _util.fix_sequence_arg(size, n, "size", int)
+    origins = _util.fix_sequence_arg(origin, n, "origin", int)
+    modes = _util.fix_sequence_arg(mode, n, "mode", _util.check_mode)
+    wdt = np.promote_types(_arrays.np_dtype(x), np.float32)
+    specs = [(ax, np.full(s, 1 / s, dtype=wdt), m, o, False)
+             for ax, s, m, o in zip(axes, sizes, modes, origins) if s > 1]
+    return _run(input, specs, output, cval, algorithm)
+
+
+# ------------------------------------------------------------- gaussian
+
+def _gaussian_kernel1d(sigma, order, radius, dtype=np.float64):
+    """Gaussian (derivative) correlation taps, FLT:689-717.
+
+    Order 0: the normalised exp(-x^2 / (2 sigma^2)) in float64 (returned as
+    float64 whatever `dtype` says, as cuCIM does). Order n: the Gaussian times
+    the polynomial q_n obtained by applying q -> q' + q * p' (p' = -x/sigma^2)
+    n times to q_0 = 1, reversed into correlation order and cast to `dtype`.
+    The numpy expressions are evaluated in the same order as cuCIM's so the
+    float64 taps are identical.
+    """
+    if order < 0:
+        raise ValueError("order must be non-negative")
+    sigma2 = sigma * sigma
+    x = np.arange(-radius, radius + 1)
+    phi = np.exp(-0.5 / sigma2 * x**2)
+    phi /= phi.sum()
+    if order == 0:
+        return phi
+    powers = np.arange(order + 1)
+    coeffs = np.zeros(order + 1)
+    coeffs[0] = 1
+    # derivative operator on polynomial coefficients plus multiplication by p'
+    op = np.diag(powers[1:], 1) + np.diag(np.ones(order) / -sigma2, -1)
+    for _ in range(order):
+        coeffs = op.dot(coeffs)
+    qx = (x[:, None] ** powers).dot(coeffs)
+    return np.ascontiguousarray((qx * phi)[::-1], dtype=dtype)
+
+
+def _gaussian_specs(ndim, in_dtype, sigma, order, mode, truncate, radius, axes):
+    """Per-axis gaussian passes of gaussian_filter (FLT:580-686); None when
+    every sigma is below 1e-15 (the filter is then a copy)."""
+    axes = _util.check_axes(axes, ndim)
+    n = len(axes)
+    sigmas = _util.fix_sequence_arg(sigma, n, "sigma", float)
+    if n == 0 or all(s < 1e-15 for s in sigmas):
+        return None
+    orders = _util.fix_sequence_arg(order, n, "order", int)
+    modes = _util.fix_sequence_arg(mode, n, "mode", str)
+    radiuses = _util.fix_sequence_arg(radius, n, "radius")
+    truncate = float(truncate)
+    wdt = np.promote_types(np.dtype(in_dtype), np.float32)
+    cache = {}
+    specs = []
+    for i in range(n):
+        if not sigmas[i] > 1e-15:
+            continue
+        key = (sigmas[i], orders[i], radiuses[i])
+        if key not in cache:
+            r = radiuses[i]
+            if r is None:
+                r = int(truncate * float(sigmas[i]) + 0.5)
+            cache[key] = None if r <= 0 else _gaussian_kernel1d(sigmas[i], orders[i], r, wdt)
+        w = cache[key]
+        _util.check_mode(modes[i] if modes[i] != "wrap" else "grid-wrap")
+        if w is not None:
+            specs.append((axes[i], w, modes[i], 0, False))
+    return specs
+
+
+def gaussian_filter(input, sigma, order=0, output=None, mode="reflect", cval=0.0,
+                    truncate=4.0, radius=None, axes=None, *, algorithm=None):
+    """Multi-dimensional Gaussian filter (FLT:580-686)."""
+    x = _arrays.as_tensor(input)
+    specs = _gaussian_specs(x.dim(), _arrays.np_dtype(x), sigma, order, mode, truncate,
+                            radius, axes)
+    if specs is None:
+        specs = []
+    return _run(input, specs, output, cval, algorithm)
+
+
+def gaussian_filter1d(input, sigma, axis=-1, order=0, output=None, mode="reflect", cval=0.0,
+                      truncate=4.0, *, algorithm=None):
+    """One-dimensional Gaussian filter (FLT:524-577)."""
+    x = _arrays.as_tensor(input)
+    radius = int(float(truncate) * float(sigma) + 0.5)
+    wdt = np.promote_types(_arrays.np_dtype(x), np.float32)
+    w = _gaussian_kernel1d(sigma, int(order), radius, wdt)
+    return correlate1d(input, w, axis, output, mode, cval, algorithm=algorithm)
+
+
+# ------------------------------------------------------------ sobel/prewitt
+
+def _prewitt_or_sobel(input, axis, output, mode, cval, smooth, algorithm):
+    """FLT:782-803: [-1, 0, 1] along `axis`, `smooth` along the others."""
+    x = _arrays.as_tensor(input)
+    axis = _util.normalize_axis(axis, x.dim())
+    wdt = np.promote_types(_arrays.np_dtype(x), np.float32)
+    diff = np.array([-1, 0, 1], dtype=wdt)
+    specs = [(a, diff if a == axis else smooth, mode, 0, False) for a in range(x.dim())]
+    for m in {mode}:
+        _util.check_mode(m)
+    return _run(input, specs, output, cval, algorithm)
+
+
+def sobel(input, axis=-1, output=None, mode="reflect", cval=0.0, *, algorithm=None):
+    """Sobel filter along `axis` (FLT:751-779)."""
+    x = _arrays.as_tensor(input)
+    wdt = np.promote_types(_arrays.np_dtype(x), np.float32)
+    return _prewitt_or_sobel(input, axis, output, mode, cval, np.array([1, 2, 1], dtype=wdt),
+                             algorithm)
+
+
+def prewitt(input, axis=-1, output=None, mode="reflect", cval=0.0, *, algorithm=None):
+    """Prewitt filter along `axis` (FLT:720-748)."""
+    x = _arrays.as_tensor(input)
+    wdt = np.promote_types(_arrays.np_dtype(x), np.float32)
+    return _prewitt_or_sobel(input, axis, output, mode, cval, np.ones(3, dtype=wdt), algorithm)
+
+
+# ------------------------------------------------------ gradient magnitude
+
+def _gradient_magnitude(input, chains, output, cval, algorithm=None):
+    """sqrt(sum over chains of chain(input)^2), FLT:1012-1097 rounding."""
+    x = _arrays.as_tensor(input)
+    xc = x.contiguous()
+    slot = _arrays.output_slot(output, input, xc)
+    out_dt = slot.dtype
+    if out_dt.kind != "f" or out_dt.itemsize < 4:
+        raise NotImplementedError("gradient magnitude supports float32/float64 outputs only")
+    lens = {len(c) for c in chains}
+    if len(lens) != 1:
+        raise RuntimeError("gradient chains must have equal length")
+    pl = _PassList()
+    for chain in chains:
+        sub = _build_passes(_arrays.np_dtype(xc), out_dt, xc.dim(), chain, cval, algorithm)
+        pl.keep += sub.keep
+        pl.items += sub.items
+    arr = pl.array()
+    a_in = _arrays.to_cimx(xc)
+    a_out = _arrays.to_cimx(slot.work)
+    rc = _lib.lib.cimx_gradient_magnitude(ctypes.byref(a_in), ctypes.byref(a_out), arr,
+                                          len(chains), lens.pop(), _arrays.stream_of(xc))
+    _lib.check(rc, "gradient magnitude")
+    return slot.result()
+
+
+def generic_gradient_magnitude(input, derivative, output=None, mode="reflect", cval=0.0,
+                               extra_arguments=(), extra_keywords=None, *, axes=None):
+    """FLT:1012-1097 with a user-supplied derivative callable."""
+    if extra_keywords is None:
+        extra_keywords = {}
+    x = _arrays.as_tensor(input)
+    ndim = x.dim()
+    axes = _util.check_axes(axes, ndim)
+    modes = _util.fix_sequence_arg(mode, len(axes), "mode", _util.check_mode)
+    slot = _arrays.output_slot(output, input, x.contiguous())
+    if ndim == 0:
+        slot.work.copy_(x)
+        return slot.result()
+    if slot.dtype.kind != "f":
+        raise NotImplementedError("generic_gradient_magnitude supports float outputs only")
+    res = _arrays.as_tensor(derivative(input, axes[0], slot.work, modes[0], cval,
+                                       *extra_arguments, **extra_keywords))
+    acc = slot.work
+    if res.data_ptr() != acc.data_ptr():
+        acc.copy_(res)
+    acc.mul_(acc)
+    if len(axes) > 1:
+        tmp = torch.empty_like(acc)
+        for i in range(1, len(axes)):
+            r = _arrays.as_tensor(derivative(input, axes[i], tmp, modes[i], cval,
+                                             *extra_arguments, **extra_keywords))
+            if r.data_ptr() != tmp.data_ptr():
+                tmp.copy_(r)
+            tmp.mul_(tmp)
+            acc.add_(tmp)
+    acc.sqrt_()
+    return slot.result()
+
+
+def gaussian_gradient_magnitude(input, sigma, output=None, mode="reflect", cval=0.0, *,
+                                axes=None, algorithm=None, **kwargs):
+    """Gradient magnitude with Gaussian derivatives (FLT:1100-1157)."""
+    x = _arrays.as_tensor(input)
+    ndim = x.dim()
+    axes = _util.check_axes(axes, ndim)
+    modes = _util.fix_sequence_arg(mode, len(axes), "mode", _util.check_mode)
+    truncate = kwargs.pop("truncate", 4.0)
+    radius = kwargs.pop("radius", None)
+    if kwargs:
+        raise TypeError(f"unexpected keyword arguments {sorted(kwargs)}")
+    chains = []
+    for ax, m in zip(axes, modes):
+        order = [0] * ndim
+        order[ax] = 1
+        specs = _gaussian_specs(ndim, _arrays.np_dtype(x), sigma, order, m, truncate, radius,
+                                None)
+        chains.append(specs if specs is not None else [])
+    return _gradient_magnitude(input, chains, output, cval, algorithm)

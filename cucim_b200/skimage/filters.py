@@ -1,0 +1,142 @@
+"""gaussian, sobel, prewitt and frangi of cucim.skimage.filters
+(python/cucim/src/cucim/skimage/_shared/filters.py:21-166,
+filters/edges.py:148-330 and :494, filters/ridges.py:228-476)."""
+
+import ctypes
+import math
+from collections.abc import Iterable
+
+import numpy as np
+import torch
+
+from .. import _arrays, _lib
+from .. import ndimage as ndi
+from .._util import check_mode, supported_float_type
+from . import util as _u
+from .feature import _hessian_matrix_with_gaussian, symmetric_compute_eigenvalues
+
+__all__ = ["gaussian", "sobel", "prewitt", "frangi"]
+
+
+def gaussian(image, sigma=1, mode="nearest", cval=0, preserve_range=False, truncate=4.0, *,
+             channel_axis=None, out=None):
+    """_shared/filters.py:21-166."""
+    msg = "Sigma values less than zero are not valid"
+    if not isinstance(sigma, Iterable):
+        if sigma < 0:
+            raise ValueError(msg)
+    elif any(s < 0 for s in sigma):
+        raise ValueError(msg)
+    x = _arrays.as_tensor(image)
+    if channel_axis is not None:
+        axes = tuple(ax for ax in range(x.dim()) if ax != channel_axis % x.dim())
+    else:
+        axes = tuple(range(x.dim()))
+    image_f = _u.convert_to_float(image, preserve_range)
+    fdt = supported_float_type(_arrays.np_dtype(_arrays.as_tensor(image_f)))
+    image_f = _u.astype(image_f, fdt)
+    if out is None:
+        return ndi.gaussian_filter(image_f, sigma, output=fdt, mode=mode, cval=cval,
+                                   truncate=truncate, axes=axes)
+    out_t = _arrays.as_tensor(out)
+    if not out_t.dtype.is_floating_point:
+        raise ValueError(f"dtype of `out` must be floating point; got {out_t.dtype!r}.")
+    ndi.gaussian_filter(image_f, sigma, output=out, mode=mode, cval=cval, truncate=truncate,
+                        axes=axes)
+    return out
+
+
+_SOBEL_SMOOTH = np.array([1, 2, 1]) / 4
+_PREWITT_SMOOTH = np.full((3,), 1 / 3)
+
+
+def _generic_edge_filter(image, *, smooth_weights, edge_weights=(1, 0, -1), axis=None,
+                         mode="reflect", cval=0.0):
+    """edges.py:148-241: the edge taps along each requested axis, the
+    smoothing taps along every other axis (ascending), all as convolutions
+    with float intermediates; with several axes the result is
+    sqrt(sum of squares) with the edge taps divided by sqrt(ndim). `cval` is
+    accepted and ignored, as in cuCIM."""
+    x = _arrays.as_tensor(image)
+    ndim = x.dim()
+    if axis is None:
+        axes = list(range(ndim))
+    elif np.isscalar(axis):
+        axes = [axis]
+    else:
+        axes = list(axis)
+    magnitude = len(axes) > 1
+    dt = _arrays.np_dtype(x)
+    if dt.kind == "f":
+        fdt = supported_float_type(dt)
+        image = _u.astype(image, fdt)
+    else:
+        image = _u.img_as_float(image)
+        fdt = _arrays.np_dtype(_arrays.as_tensor(image))
+    ew = np.asarray(edge_weights, dtype=fdt)
+    sw = np.asarray(smooth_weights, dtype=fdt)
+    if magnitude:
+        ew = (ew / fdt.type(math.sqrt(ndim))).astype(fdt)
+    if not isinstance(mode, str):
+        raise RuntimeError(f"boundary mode not supported (actual: {mode})")
+    check_mode(mode)
+    chains = []
+    for ed in axes:
+        ed_n = ed % ndim
+        chain = [(ed_n, ew, mode, 0, True)]
+        chain += [(sd, sw, mode, 0, True) for sd in sorted(set(range(ndim)) - {ed_n})]
+        chains.append(chain)
+    if magnitude:
+        return ndi._gradient_magnitude(image, chains, fdt, 0.0)
+    return ndi._run(image, chains[0], fdt, 0.0)
+
+
+def _mask_unsupported(mask):
+    if mask is not None:
+        raise NotImplementedError("mask is not supported on this path")
+
+
+def sobel(image, mask=None, *, axis=None, mode="reflect", cval=0.0):
+    """edges.py:244-306."""
+    _mask_unsupported(mask)
+    return _generic_edge_filter(image, smooth_weights=_SOBEL_SMOOTH, axis=axis, mode=mode,
+                                cval=cval)
+
+
+def prewitt(image, mask=None, *, axis=None, mode="reflect", cval=0.0):
+    """edges.py:494-553."""
+    _mask_unsupported(mask)
+    return _generic_edge_filter(image, smooth_weights=_PREWITT_SMOOTH, axis=axis, mode=mode,
+                                cval=cval)
+
+
+def frangi(image, sigmas=range(1, 10, 2), scale_range=None, scale_step=None, alpha=0.5,
+           beta=0.5, gamma=None, black_ridges=True, mode="reflect", cval=0):
+    """ridges.py:322-476. The automatic gamma (half the largest Hessian norm
+    of the first scale) stays on the device: no host synchronisation."""
+    if scale_range is not None and scale_step is not None:
+        sigmas = np.arange(scale_range[0], scale_range[1], scale_step)
+    x = _arrays.as_tensor(image)
+    if x.dim() not in (2, 3):
+        raise ValueError(
+            f"The parameter `image` must be a 2-dimensional or 3-dimensional array")
+    fdt = supported_float_type(_arrays.np_dtype(x))
+    if black_ridges:
+        image = _u.astype(image, fdt)
+    else:
+        image = _u.negative_astype(image, fdt)
+    ndim = x.dim()
+    out = _arrays.empty(x.shape, fdt, x.device)
+    state = torch.zeros(1, dtype=torch.int64, device=x.device)
+    g = float("nan") if gamma is None else float(gamma)
+    a_out = _arrays.to_cimx(out)
+    for i, sigma in enumerate(sigmas):
+        H = _hessian_matrix_with_gaussian(image, sigma, mode=mode, cval=cval)
+        ev = _arrays.as_tensor(symmetric_compute_eigenvalues(H, sort="ascending", abs_sort=True))
+        eigs = (_lib.CimxArray * ndim)(*[_arrays.to_cimx(ev[k]) for k in range(ndim)])
+        rc = _lib.lib.cimx_frangi_accumulate(eigs, ndim, ctypes.byref(a_out), float(alpha),
+                                             float(beta), g, 1 if i == 0 else 0,
+                                             ctypes.c_void_p(state.data_ptr()),
+                                             _arrays.stream_of(out))
+        _lib.check(rc, "frangi")
+    return _arrays.wrap_like(image, out)

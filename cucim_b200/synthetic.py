@@ -1,0 +1,105 @@
+"""Seeded synthetic inputs for the filtering workloads.
+
+No public dataset is involved; these generators produce images with the
+shapes, dtypes and value distributions of the standard workloads:
+
+- ``uniform_image``: float32 i.i.d. uniform [0, 1) (2-D gaussian workload);
+- ``smooth_volume_u16``: uint16 stack made by smoothing normal noise
+  (sigma 3), rescaling to [0, 65535] and adding Poisson shot noise;
+- ``rectangles_image``: float32 uniform [0, 1) plus axis-aligned rectangles
+  of constant value in [0, 10) (large-kernel precision workload);
+- ``rgb_tiles``: uint8 RGB tiles of random sizes with per-channel
+  three-component Gaussian-mixture values, plus a sigma per tile;
+- ``segments_volume``: float32 volume of random line segments with Gaussian
+  cross-sections on N(0, 0.05) noise (vesselness workload).
+"""
+
+import math
+
+import numpy as np
+
+
+def uniform_image(shape=(2048, 2048), seed=0):
+    return np.random.default_rng(seed).random(shape, dtype=np.float32)
+
+
+def smooth_volume_u16(shape=(512, 1024, 1024), seed=1, smooth=None):
+    """`smooth(x, sigma)` smooths a float32 array (default: scipy.ndimage,
+    mode 'reflect'); pass the GPU filter for large volumes."""
+    rng = np.random.default_rng(seed)
+    noise = rng.standard_normal(shape, dtype=np.float32)
+    if smooth is None:
+        import scipy.ndimage as sndi  # noqa: PLC0415
+
+        sm = sndi.gaussian_filter(noise, 3.0, mode="reflect")
+    else:
+        sm = np.asarray(smooth(noise, 3.0), dtype=np.float32)
+    lo, hi = float(sm.min()), float(sm.max())
+    scaled = (sm - lo) * (65535.0 / max(hi - lo, 1e-30))
+    shot = rng.poisson(np.clip(scaled, 0, None).astype(np.float64))
+    return np.clip(shot, 0, 65535).astype(np.uint16)
+
+
+def rectangles_image(shape=(8192, 8192), n_rect=64, seed=2):
+    rng = np.random.default_rng(seed)
+    img = rng.random(shape, dtype=np.float32)
+    for _ in range(n_rect):
+        y = np.sort(rng.integers(0, shape[0], 2))
+        x = np.sort(rng.integers(0, shape[1], 2))
+        img[y[0]:y[1] + 1, x[0]:x[1] + 1] = np.float32(rng.uniform(0, 10))
+    return img
+
+
+def rgb_tiles(n_tiles=4096, side_range=(64, 1024), seed=3, sigma_range=(0.5, 8.0)):
+    """List of (H, W, 3) uint8 tiles and a float sigma per tile."""
+    rng = np.random.default_rng(seed)
+    means = np.array([60.0, 150.0, 220.0])
+    tiles, sigmas = [], []
+    for _ in range(n_tiles):
+        h, w = rng.integers(side_range[0], side_range[1] + 1, 2)
+        comp = rng.integers(0, 3, size=(h, w, 3))
+        vals = rng.normal(means[comp], 20.0)
+        tiles.append(np.clip(np.rint(vals), 0, 255).astype(np.uint8))
+        sigmas.append(float(rng.uniform(*sigma_range)))
+    return tiles, sigmas
+
+
+def segments_volume(shape=(256, 256, 256), n_segments=200, seed=4,
+                    length_range=(20, 120), radius_range=(1.0, 4.0)):
+    rng = np.random.default_rng(seed)
+    vol = rng.normal(0.0, 0.05, size=shape).astype(np.float32)
+    dims = np.array(shape)
+    for _ in range(n_segments):
+        p0 = rng.uniform(0, dims)
+        d = rng.normal(size=3)
+        d /= np.linalg.norm(d)
+        length = rng.uniform(*length_range)
+        sig = rng.uniform(*radius_range)
+        p1 = p0 + d * length
+        reach = 4 * sig
+        lo = np.maximum(np.floor(np.minimum(p0, p1) - reach).astype(int), 0)
+        hi = np.minimum(np.ceil(np.maximum(p0, p1) + reach).astype(int) + 1, dims)
+        if np.any(hi <= lo):
+            continue
+        zz, yy, xx = np.meshgrid(*[np.arange(lo[i], hi[i]) for i in range(3)], indexing="ij")
+        pts = np.stack([zz, yy, xx], -1).astype(np.float64)
+        t = np.clip(((pts - p0) @ d) / length, 0.0, 1.0)
+        closest = p0 + (t[..., None] * length) * d
+        d2 = ((pts - closest) ** 2).sum(-1)
+        vol[lo[0]:hi[0], lo[1]:hi[1], lo[2]:hi[2]] += np.exp(
+            -d2 / (2 * sig * sig)).astype(np.float32)
+    return vol
+
+
+def gaussian_radius(sigma, truncate=4.0):
+    return int(truncate * float(sigma) + 0.5)
+
+
+def taps_count(sigma, truncate=4.0):
+    return 2 * gaussian_radius(sigma, truncate) + 1
+
+
+__all__ = [
+    "uniform_image", "smooth_volume_u16", "rectangles_image", "rgb_tiles", "segments_volume",
+    "gaussian_radius", "taps_count", "math",
+]

@@ -1,0 +1,182 @@
+/*
+ * cimx.h — C ABI of libcimx.so, the B200 (sm_100a) separable n-D filtering
+ * library behind the cucim_b200 Python package.
+ *
+ * Every entry point takes plain pointers and sizes, enqueues its work on the
+ * CUDA stream it is given (a cudaStream_t passed as void*, NULL = legacy
+ * default stream) and returns 0 on success or a negative CIMX_E* code.
+ * cimx_last_error_string() describes the last failure on the calling thread.
+ * Nothing here synchronises the stream unless the comment says so.
+ *
+ * The arithmetic each entry performs is the arithmetic of the cuCIM code it
+ * replaces (paths are relative to python/cucim/src/cucim/skimage in
+ * rapidsai/cucim):
+ *   - taps are applied in ascending order as one fused multiply-add chain
+ *     per output, sum = fma(x[k], w[k], sum), starting from +0, in the
+ *     weights type W (float32 or float64);
+ *   - the result is stored with cuCIM's cast<D>() rule
+ *     (_vendored/_ndimage_filters_core.py:227-244);
+ *   - boundary modes follow _vendored/_ndimage_util.py:186-308.
+ */
+#ifndef CIMX_H_
+#define CIMX_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define CIMX_API __attribute__((visibility("default")))
+#else
+#define CIMX_API
+#endif
+
+#define CIMX_MAX_NDIM 8
+
+/* Element types: the numpy dtype.char of the array ('B','b','H','h','I','i',
+ * 'L'/'Q','l'/'q','e','f','d'). */
+typedef struct CimxArray {
+  void* data;                       /* device pointer */
+  int32_t dtype;                    /* numpy dtype.char, e.g. 'f' */
+  int32_t ndim;                     /* 0..CIMX_MAX_NDIM */
+  int64_t shape[CIMX_MAX_NDIM];
+  int64_t strides[CIMX_MAX_NDIM];   /* bytes */
+} CimxArray;
+
+/* Boundary modes (filters map 'wrap' to 'grid-wrap' before calling). */
+enum {
+  CIMX_MODE_REFLECT = 0,   /* 'reflect' == 'grid-mirror'  (d c b a | a b c d | d c b a) */
+  CIMX_MODE_MIRROR = 1,    /* 'mirror'                    (d c b | a b c d | c b a)   */
+  CIMX_MODE_NEAREST = 2,   /* 'nearest'                   (a a a | a b c d | d d d)   */
+  CIMX_MODE_GRID_WRAP = 3, /* 'grid-wrap' (and 'wrap' for filters) (a b c d | a b c d) */
+  CIMX_MODE_CONSTANT = 4,  /* 'constant'                  (k k k | a b c d | k k k)   */
+};
+
+/* Per-pass flags. */
+enum {
+  CIMX_F_W64 = 1 << 0,          /* weights type W is float64 (else float32) */
+  CIMX_F_CONVOLVE = 1 << 1,     /* taps are applied reversed (convolve1d) */
+  CIMX_F_CVAL_AS_INPUT = 1 << 2,/* constant mode: halo value is (W)(T)cval as in the
+                                   shared-memory kernel (filters/_separable_filtering.py:219-223);
+                                   otherwise (W)cval as in the elementwise kernel
+                                   (_vendored/_ndimage_filters_core.py:334-348) */
+  CIMX_F_SKIP_ZERO_TAPS = 1 << 3,/* zero taps are skipped, as the elementwise kernel does
+                                   (_vendored/_ndimage_filters_core.py:307-309) */
+};
+
+/* Library-level flags for multi-pass calls. */
+enum {
+  CIMX_L_NO_FUSION = 1 << 0,    /* force one launch per pass (ping-pong through scratch) */
+};
+
+/* One 1-D correlation pass of a separable filter. */
+typedef struct CimxPass {
+  int32_t axis;        /* axis of the input it runs along */
+  int32_t ntaps;       /* K >= 1 */
+  int32_t origin;      /* cuCIM origin; anchor = K/2 + origin (after the convolve flip) */
+  int32_t mode;        /* CIMX_MODE_* */
+  double cval;         /* constant-mode fill value as given by the caller */
+  int32_t flags;       /* CIMX_F_* */
+  int32_t reserved;
+  const double* taps;  /* host pointer to K taps (rounded to W inside) */
+} CimxPass;
+
+/* Error codes. */
+enum {
+  CIMX_OK = 0,
+  CIMX_E_INVALID = -1,     /* bad argument (shape, axis, mode, ntaps, origin) */
+  CIMX_E_DTYPE = -2,       /* unsupported element type */
+  CIMX_E_CUDA = -3,        /* a CUDA call failed */
+  CIMX_E_NOMEM = -4,       /* scratch allocation failed */
+  CIMX_E_LAYOUT = -5,      /* array is not C-contiguous where required */
+  CIMX_E_TIMEOUT = -6,     /* a bounded device-side wait gave up */
+};
+
+/* Version of this ABI (major*100 + minor). */
+CIMX_API int cimx_abi_version(void);
+
+/* Description of the last error raised on the calling thread. */
+CIMX_API const char* cimx_last_error_string(void);
+
+/* Scratch allocator hook (default: cudaMallocAsync / cudaFreeAsync on the
+ * call's stream). Both functions receive the stream the call runs on. */
+typedef void* (*cimx_alloc_fn)(size_t nbytes, void* stream, void* user);
+typedef void (*cimx_free_fn)(void* ptr, size_t nbytes, void* stream, void* user);
+CIMX_API int cimx_set_allocator(cimx_alloc_fn alloc, cimx_free_fn release, void* user);
+
+/* One 1-D correlation (or convolution) along `axis`.
+ * Replaces the shared-memory kernel driver _shmem_convolve1d
+ * (filters/_separable_filtering.py:977-1070) and the elementwise correlate
+ * kernel call (_vendored/_ndimage_filters.py:224-257 -> _vendored/_ndimage_filters_core.py:166-214).
+ * `in` and `out` must be C-contiguous with equal shapes and must not overlap. */
+CIMX_API int cimx_correlate1d(const CimxArray* in, const CimxArray* out, const double* taps,
+                     int ntaps, int axis, int origin, int mode, double cval,
+                     int flags, void* stream);
+
+/* A sequence of 1-D passes applied in order, intermediates stored in the
+ * output's dtype exactly like _run_1d_filters
+ * (_vendored/_ndimage_filters_core.py:124-163). Consecutive passes are fused
+ * into one launch when the shapes allow it; the result is bit-identical to
+ * running them one by one. Scratch (one temporary of the output's shape and
+ * dtype) is taken from the allocator only when passes are not fused.
+ * Used by gaussian_filter, uniform_filter, sobel, prewitt
+ * (_vendored/_ndimage_filters.py:363-396, 447-521, 580-686, 720-803). */
+CIMX_API int cimx_separable(const CimxArray* in, const CimxArray* out, const CimxPass* passes,
+                   int npasses, int lib_flags, void* stream);
+
+/* out = sqrt(sum_i d_i^2) with d_i = separable(in, passes[i*passes_per_axis ...]),
+ * i = 0..naxes-1, with cuCIM's rounding order: out = d_0*d_0 (rounded),
+ * then out += (d_i*d_i rounded) for i >= 1, then sqrt. Replaces
+ * generic_gradient_magnitude as driven by gaussian_gradient_magnitude
+ * (_vendored/_ndimage_filters.py:1012-1097, :1100-1157) and the magnitude
+ * branch of the skimage edge filters (filters/edges.py:148-241, where each
+ * chain is the edge pass followed by the smoothing passes).
+ * `out` must be float32 or float64. */
+CIMX_API int cimx_gradient_magnitude(const CimxArray* in, const CimxArray* out,
+                            const CimxPass* passes, int naxes, int passes_per_axis,
+                            void* stream);
+
+/* Closed-form eigenvalues of symmetric 2x2 / 3x3 matrices given as the
+ * upper-triangular element images in row-major order ((00,01,11) or
+ * (00,01,02,11,12,22)). `out` holds nelems==3 ? 2 : 3 images of the same
+ * shape. sort: 0 = ascending, 1 = descending; abs_sort sorts by magnitude.
+ * Follows feature/corner.py:473-527 (2x2) and :566-647 (3x3, float64 inside). */
+CIMX_API int cimx_eigvals_sym(const CimxArray* elems, int nelems, const CimxArray* out,
+                     int sort, int abs_sort, void* stream);
+
+/* rgb2gray: gray = 0.2125 R + 0.7154 G + 0.0721 B computed in float64,
+ * stored in gray's dtype; rgb is (..., 3) C-contiguous float32/float64
+ * (color/colorconv.py:1038-1095). When rgb is uint8 it is first scaled by
+ * float32(1/255) as img_as_float32 does (util/dtype.py:360-361). */
+CIMX_API int cimx_rgb2gray(const CimxArray* rgb, const CimxArray* gray, void* stream);
+
+/* Elementwise conversion into a float32/float64 array (util/dtype.py:219-372):
+ * op 0 = astype; op 1 = img_as_float (integers scaled by 1/max of their type
+ * in float32 for <= 16-bit inputs, float64 otherwise; signed results clipped
+ * at -1); op 2 = astype then negation (frangi with black_ridges=False,
+ * filters/ridges.py:411-413). */
+CIMX_API int cimx_convert(const CimxArray* in, const CimxArray* out, int op, void* stream);
+
+/* numpy.gradient along `axis` with unit spacing and edge_order=1, used by
+ * hessian_matrix(use_gaussian_derivatives=False) (feature/corner.py:370-382). */
+CIMX_API int cimx_gradient_fd(const CimxArray* in, const CimxArray* out, int axis, void* stream);
+
+/* One scale of frangi's epilogue (filters/ridges.py:228-319 and :436-475):
+ * from the eigenvalues (sorted ascending by magnitude) compute the vesselness
+ * and store it (first != 0) or fold it into `out` with a NaN-propagating
+ * maximum. gamma = NaN selects cuCIM's automatic gamma: half the square root
+ * of the largest sum of squared eigenvalues of the first scale, kept on the
+ * device in *gamma_state (8 bytes of device memory owned by the caller); no
+ * host synchronisation is needed. */
+CIMX_API int cimx_frangi_accumulate(const CimxArray* eigs, int ndim, const CimxArray* out,
+                                    double alpha, double beta, double gamma, int first,
+                                    void* gamma_state, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CIMX_H_ */

@@ -1,0 +1,295 @@
+/*
+ * cimx_oracle.c — TEST INFRASTRUCTURE ONLY (the parity oracle).
+ *
+ * A plain-C CPU restatement of the per-output arithmetic of cuCIM's
+ * separable correlation kernels. Only tests/, __graft_entry__.smoke() and
+ * bench.py's CPU baseline use it; the product never calls it.
+ *
+ * What it restates (paths relative to python/cucim/src/cucim/skimage):
+ *   - boundary index maps: _vendored/_ndimage_util.py:186-308
+ *     (reflect/grid-mirror :196-217, mirror :218-247, nearest :248-255,
+ *      grid-wrap :256-274, constant :290-307 with the fill value applied as in
+ *      _vendored/_ndimage_filters_core.py:334-348 and
+ *      filters/_separable_filtering.py:219-223);
+ *   - the tap loop: k ascending, sum = sum + (W)x * w[k] contracted to a fused
+ *     multiply-add (filters/_separable_filtering.py:728-747 and
+ *     _vendored/_ndimage_filters.py:347-360 via
+ *     _vendored/_ndimage_filters_core.py:307-309, which also skips zero taps);
+ *   - the output cast cast<D>(sum): _vendored/_ndimage_filters_core.py:227-244,
+ *     with the saturating float->integer conversion of the GPU
+ *     (cvt.rzi; 8-bit results go through a saturating 16-bit conversion and
+ *     are then truncated, which is how the CUDA compiler lowers an 8-bit cast).
+ *
+ * fmaf()/fma() from libm are correctly rounded, so the chain is the exact
+ * IEEE fused chain the GPU runs. Build with -ffp-contract=off so that no
+ * other expression gets contracted.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <string.h>
+
+enum { M_REFLECT = 0, M_MIRROR = 1, M_NEAREST = 2, M_GRID_WRAP = 3, M_CONSTANT = 4 };
+
+static inline int64_t map_index(int64_t ix, int64_t n, int mode) {
+  switch (mode) {
+    case M_REFLECT:
+      if (ix < 0) ix = -1 - ix;
+      ix %= 2 * n;
+      if (2 * n - 1 - ix < ix) ix = 2 * n - 1 - ix;
+      return ix;
+    case M_MIRROR:
+      if (n == 1) return 0;
+      if (ix < 0) ix = -ix;
+      ix = 1 + (ix - 1) % ((n - 1) * 2);
+      if (2 * n - 2 - ix < ix) ix = 2 * n - 2 - ix;
+      return ix;
+    case M_NEAREST:
+      if (ix < 0) return 0;
+      if (ix > n - 1) return n - 1;
+      return ix;
+    case M_GRID_WRAP:
+      ix %= n;
+      if (ix < 0) ix += n;
+      return ix;
+    default: /* constant */
+      return (ix < 0 || ix >= n) ? -1 : ix;
+  }
+}
+
+/* ---- element access ------------------------------------------------------ */
+
+static float half_to_float(uint16_t h) {
+  uint32_t s = (uint32_t)(h >> 15) << 31;
+  uint32_t e = (h >> 10) & 0x1f, m = h & 0x3ff, bits;
+  if (e == 0) {
+    if (m == 0) {
+      bits = s;
+    } else { /* subnormal */
+      int sh = 0;
+      while (!(m & 0x400)) { m <<= 1; ++sh; }
+      m &= 0x3ff;
+      bits = s | ((uint32_t)(127 - 15 - sh + 1) << 23) | (m << 13);
+    }
+  } else if (e == 31) {
+    bits = s | 0x7f800000u | (m << 13);
+  } else {
+    bits = s | ((e - 15 + 127) << 23) | (m << 13);
+  }
+  float f;
+  memcpy(&f, &bits, 4);
+  return f;
+}
+
+/* round-to-nearest-even float -> half */
+static uint16_t float_to_half(float f) {
+  uint32_t x;
+  memcpy(&x, &f, 4);
+  uint32_t s = (x >> 16) & 0x8000u;
+  uint32_t ax = x & 0x7fffffffu;
+  if (ax >= 0x7f800000u) return (uint16_t)(s | 0x7c00u | (ax > 0x7f800000u ? 0x200u : 0));
+  if (ax >= 0x477ff000u) return (uint16_t)(s | 0x7c00u); /* overflow to inf */
+  if (ax < 0x38800000u) { /* subnormal or zero in half */
+    float a;
+    memcpy(&a, &ax, 4);
+    /* half subnormal unit is 2^-24: scale and round to nearest even */
+    float q = a * 16777216.0f; /* exact */
+    float r = nearbyintf(q);
+    return (uint16_t)(s | (uint32_t)r);
+  }
+  uint32_t mant = ax & 0x7fffffu;
+  int32_t e = (int32_t)(ax >> 23) - 127 + 15;
+  uint32_t hm = mant >> 13, rem = mant & 0x1fffu;
+  uint32_t h = ((uint32_t)e << 10) | hm;
+  if (rem > 0x1000u || (rem == 0x1000u && (hm & 1))) h += 1;
+  return (uint16_t)(s | h);
+}
+
+static inline double load_d(const void* p, int dt, int64_t i) {
+  switch (dt) {
+    case 'B': return (double)((const uint8_t*)p)[i];
+    case 'b': return (double)((const int8_t*)p)[i];
+    case '?': return (double)((const uint8_t*)p)[i];
+    case 'H': return (double)((const uint16_t*)p)[i];
+    case 'h': return (double)((const int16_t*)p)[i];
+    case 'I': return (double)((const uint32_t*)p)[i];
+    case 'i': return (double)((const int32_t*)p)[i];
+    case 'L': case 'Q': return (double)((const uint64_t*)p)[i];
+    case 'l': case 'q': return (double)((const int64_t*)p)[i];
+    case 'e': return (double)half_to_float(((const uint16_t*)p)[i]);
+    case 'f': return (double)((const float*)p)[i];
+    default: return ((const double*)p)[i];
+  }
+}
+
+/* (float)x for every T, converting directly from T (no double rounding). */
+static inline float load_f(const void* p, int dt, int64_t i) {
+  switch (dt) {
+    case 'L': case 'Q': return (float)((const uint64_t*)p)[i];
+    case 'l': case 'q': return (float)((const int64_t*)p)[i];
+    case 'd': return (float)((const double*)p)[i];
+    default: return (float)load_d(p, dt, i);
+  }
+}
+
+/* static_cast<T>(cval) followed by (W): the shared-memory kernel's fill value. */
+double oracle_cval_as_input(double cval, int dt, int w64);
+
+/* GPU float->integer conversion: truncate toward zero, saturate to
+ * [lo, hi], NaN -> 0. */
+static inline double sat_trunc(double a, double lo, double hi) {
+  if (a != a) return 0.0;
+  a = trunc(a);
+  if (a < lo) return lo;
+  if (a > hi) return hi;
+  return a;
+}
+
+/* Conversion of a float/double value `a` to integer type dt as the CUDA
+ * compiler lowers a C cast (8-bit targets: saturating 16-bit conversion, then
+ * truncation to 8 bits). Returns the integer as a 64-bit pattern. */
+static inline uint64_t c_cast_int(double a, int dt) {
+  switch (dt) {
+    case 'B': case 'b': case '?': {
+      int64_t v = (int64_t)sat_trunc(a, -32768.0, 32767.0);
+      return (uint64_t)(uint8_t)v;
+    }
+    case 'H': return (uint64_t)(uint16_t)(int64_t)sat_trunc(a, 0.0, 65535.0);
+    case 'h': return (uint64_t)(uint16_t)(int16_t)(int64_t)sat_trunc(a, -32768.0, 32767.0);
+    case 'I': return (uint64_t)(uint32_t)(int64_t)sat_trunc(a, 0.0, 4294967295.0);
+    case 'i': return (uint64_t)(uint32_t)(int32_t)(int64_t)sat_trunc(a, -2147483648.0, 2147483647.0);
+    case 'L': case 'Q': {
+      if (a != a || a <= 0) return 0;
+      if (a >= 18446744073709551616.0) return UINT64_MAX;
+      return (uint64_t)trunc(a);
+    }
+    default: { /* int64 */
+      if (a != a) return 0;
+      if (a >= 9223372036854775808.0) return (uint64_t)INT64_MAX;
+      if (a < -9223372036854775808.0) return (uint64_t)INT64_MIN;
+      return (uint64_t)(int64_t)trunc(a);
+    }
+  }
+}
+
+static inline int is_unsigned(int dt) {
+  return dt == 'B' || dt == 'H' || dt == 'I' || dt == 'L' || dt == 'Q' || dt == '?';
+}
+
+static inline void store_bits(void* p, int dt, int64_t i, uint64_t v) {
+  switch (dt) {
+    case 'B': case 'b': case '?': ((uint8_t*)p)[i] = (uint8_t)v; break;
+    case 'H': case 'h': ((uint16_t*)p)[i] = (uint16_t)v; break;
+    case 'I': case 'i': ((uint32_t*)p)[i] = (uint32_t)v; break;
+    default: ((uint64_t*)p)[i] = v; break;
+  }
+}
+
+/* cast<D>(a) of _vendored/_ndimage_filters_core.py:227-244 with a in W. */
+static inline void store_cast(void* p, int dt, int64_t i, double a, int w64) {
+  switch (dt) {
+    case 'f': ((float*)p)[i] = (float)a; return;
+    case 'd': ((double*)p)[i] = a; return;
+    case 'e': ((uint16_t*)p)[i] = float_to_half((float)a); return;
+    default: break;
+  }
+  (void)w64;
+  if (is_unsigned(dt)) {
+    /* (a >= 0) ? (B)a : -(B)(-a) */
+    if (a >= 0) {
+      store_bits(p, dt, i, c_cast_int(a, dt));
+    } else {
+      uint64_t v = c_cast_int(-a, dt);
+      store_bits(p, dt, i, (uint64_t)(0 - v));
+    }
+  } else {
+    store_bits(p, dt, i, c_cast_int(a, dt));
+  }
+}
+
+double oracle_cval_as_input(double cval, int dt, int w64) {
+  double t;
+  switch (dt) {
+    case 'f': t = (double)(float)cval; break;
+    case 'd': t = cval; break;
+    case 'e': t = (double)half_to_float(float_to_half((float)cval)); break;
+    default: {
+      /* static_cast<T>(double) for an integer T (saturating, NaN -> 0). */
+      uint64_t bits = c_cast_int(cval, dt);
+      switch (dt) {
+        case 'B': case '?': t = (double)(uint8_t)bits; break;
+        case 'b': t = (double)(int8_t)bits; break;
+        case 'H': t = (double)(uint16_t)bits; break;
+        case 'h': t = (double)(int16_t)bits; break;
+        case 'I': t = (double)(uint32_t)bits; break;
+        case 'i': t = (double)(int32_t)bits; break;
+        case 'L': case 'Q': t = w64 ? (double)bits : (double)(float)bits; break;
+        default: t = w64 ? (double)(int64_t)bits : (double)(float)(int64_t)bits; break;
+      }
+    }
+  }
+  return w64 ? t : (double)(float)t;
+}
+
+/*
+ * One 1-D pass over the C-contiguous view (outer, L, inner) of `in`, along
+ * the middle axis. taps[] hold the K weights already rounded to W (and
+ * already reversed for a convolution); anchor = K/2 + origin; cval_w is the
+ * fill value as a W value. threads > 1 splits the lines with OpenMP.
+ */
+void oracle_correlate1d(const void* in, int tin, void* out, int tout, int64_t outer,
+                        int64_t L, int64_t inner, const double* taps, int K, int anchor,
+                        int mode, double cval_w, int w64, int skip_zero, int threads) {
+  const int64_t nlines = outer * inner;
+  float wf[4096];
+  int Kc = K < 4096 ? K : 4096;
+  for (int k = 0; k < Kc; ++k) wf[k] = (float)taps[k];
+#if defined(_OPENMP)
+#pragma omp parallel for schedule(static) num_threads(threads > 0 ? threads : 1)
+#else
+  (void)threads;
+#endif
+  for (int64_t line = 0; line < nlines; ++line) {
+    const int64_t o = line / inner, i = line % inner;
+    const int64_t base = o * L * inner + i;
+    for (int64_t l = 0; l < L; ++l) {
+      if (w64) {
+        double s = 0.0;
+        for (int k = 0; k < K; ++k) {
+          const double w = taps[k];
+          if (skip_zero && w == 0.0) continue;
+          const int64_t ix = map_index(l - anchor + k, L, mode);
+          double x;
+          if (ix < 0) {
+            x = cval_w;
+          } else {
+            const int64_t e = base + ix * inner;
+            if (tin == 'L' || tin == 'Q') x = (double)((const uint64_t*)in)[e];
+            else if (tin == 'l' || tin == 'q') x = (double)((const int64_t*)in)[e];
+            else x = load_d(in, tin, e);
+          }
+          s = fma(x, w, s);
+        }
+        store_cast(out, tout, base + l * inner, s, 1);
+      } else {
+        float s = 0.0f;
+        for (int k = 0; k < K; ++k) {
+          const float w = wf[k];
+          if (skip_zero && w == 0.0f) continue;
+          const int64_t ix = map_index(l - anchor + k, L, mode);
+          const float x = ix < 0 ? (float)cval_w : load_f(in, tin, base + ix * inner);
+          s = fmaf(x, w, s);
+        }
+        store_cast(out, tout, base + l * inner, (double)s, 0);
+      }
+    }
+  }
+}
+
+/* Elementwise cast of a W-typed array (float32 when w64 == 0) into dtype dt
+ * with cast<D>() semantics; used for checking the cast table alone. */
+void oracle_cast(const void* in, int w64, void* out, int tout, int64_t n) {
+  for (int64_t i = 0; i < n; ++i) {
+    const double a = w64 ? ((const double*)in)[i] : (double)((const float*)in)[i];
+    store_cast(out, tout, i, a, w64);
+  }
+}

@@ -1,0 +1,701 @@
+"""Parity oracle — TEST INFRASTRUCTURE ONLY.
+
+A CPU restatement (numpy + the C core in cimx_oracle.c) of cuCIM's separable
+filtering path: the host-side dtype rules, the choice between the
+shared-memory and elementwise kernels (which decides how a constant-mode fill
+value is rounded and whether zero taps are skipped), the per-axis ping-pong,
+and the composite operations built on it. Only tests/, the smoke check and
+bench.py's CPU baseline may import this module; the library never does.
+
+Citations are relative to python/cucim/src/cucim/skimage in rapidsai/cucim
+(cuCIM 26.10.00). FLT = _vendored/_ndimage_filters.py,
+CORE = _vendored/_ndimage_filters_core.py, UTIL = _vendored/_ndimage_util.py,
+SEP = filters/_separable_filtering.py.
+"""
+
+import ctypes
+import math
+from itertools import combinations_with_replacement
+
+import numpy as np
+
+from . import build_oracle
+
+_lib = ctypes.CDLL(build_oracle.build())
+_lib.oracle_correlate1d.argtypes = [
+    ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
+    ctypes.c_int64, ctypes.c_int64, ctypes.c_int64,
+    ctypes.POINTER(ctypes.c_double), ctypes.c_int, ctypes.c_int, ctypes.c_int,
+    ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+]
+_lib.oracle_correlate1d.restype = None
+_lib.oracle_cval_as_input.argtypes = [ctypes.c_double, ctypes.c_int, ctypes.c_int]
+_lib.oracle_cval_as_input.restype = ctypes.c_double
+_lib.oracle_cast.argtypes = [
+    ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int64,
+]
+_lib.oracle_cast.restype = None
+
+MODES = {
+    "reflect": 0, "grid-mirror": 0, "mirror": 1, "nearest": 2,
+    "grid-wrap": 3, "wrap": 3, "constant": 4,
+}
+# The mode names UTIL:95-108 accepts ('grid-reflect' passes the check but has
+# no boundary code in UTIL:186-308, so cuCIM fails on it later).
+_VALID_MODES = (
+    "reflect", "constant", "nearest", "mirror", "wrap", "grid-mirror",
+    "grid-wrap", "grid-reflect",
+)
+
+# sharedMemPerBlock on every CUDA device cuCIM targets (48 KiB, SEP:130-152).
+SHARED_BLOCK_BYTES = 49152
+
+THREADS = 1  # OpenMP threads the C core may use
+
+
+def _dchar(dt):
+    return ord(np.dtype(dt).char)
+
+
+# ---------------------------------------------------------------- dtype rules
+
+_NEW_FLOAT = {
+    "f": np.float32, "d": np.float64, "e": np.float32, "b": np.float32,
+    "B": np.float32, "h": np.float32, "H": np.float32, "?": np.float32,
+}
+
+
+def supported_float_type(dt):
+    """_shared/utils.py:1131-1179."""
+    dt = np.dtype(dt)
+    if dt.kind == "c":
+        raise ValueError("complex valued input is not supported")
+    return np.dtype(_NEW_FLOAT.get(dt.char, np.float64))
+
+
+def weights_dtype(input_dtype, w_dtype):
+    """UTIL:35-46 with use_cucim_casting=True."""
+    w_dtype = np.dtype(w_dtype)
+    if w_dtype.kind in "iub":
+        return supported_float_type(w_dtype)
+    return np.promote_types(np.dtype(input_dtype), np.float32)
+
+
+def img_as_float(image):
+    """util/dtype.py:489 -> _convert (:219), uint/int -> float branch (:355-372)."""
+    image = np.asarray(image)
+    dt = image.dtype
+    out_t = supported_float_type(dt)
+    if dt.kind == "f":
+        return image.astype(out_t) if dt != out_t else image
+    if dt.kind == "b":
+        return image.astype(out_t)
+    info = np.iinfo(dt)
+    comp = np.float32 if dt.itemsize <= 4 and out_t == np.float32 else np.float64
+    if out_t == np.float64:
+        comp = np.float64
+    scale = comp(1.0 / info.max)
+    res = np.multiply(image.astype(comp), scale, dtype=comp)
+    if dt.kind == "i":
+        res = np.maximum(res, comp(-1.0))
+    return res.astype(out_t)
+
+
+def convert_to_float(image, preserve_range):
+    """_shared/utils.py:1019-1052."""
+    image = np.asarray(image)
+    if image.dtype == np.float16:
+        return image.astype(np.float32)
+    if preserve_range:
+        if image.dtype.char not in "df":
+            image = image.astype(supported_float_type(image.dtype))
+        return image
+    return img_as_float(image)
+
+
+# ------------------------------------------------------------ argument checks
+
+def check_mode(mode):
+    """UTIL:95-108."""
+    if mode not in _VALID_MODES:
+        raise RuntimeError(f"boundary mode not supported (actual: {mode})")
+    if mode == "grid-reflect":
+        raise RuntimeError(f"boundary mode not supported (actual: {mode})")
+    return mode
+
+
+def check_origin(origin, width):
+    """UTIL:88-92."""
+    origin = int(origin)
+    if (width // 2 + origin < 0) or (width // 2 + origin >= width):
+        raise ValueError("invalid origin")
+    return origin
+
+
+def fix_sequence_arg(arg, ndim, name, conv=lambda x: x):
+    """UTIL:74-85."""
+    if isinstance(arg, str):
+        return [conv(arg)] * ndim
+    try:
+        arg = iter(arg)
+    except TypeError:
+        return [conv(arg)] * ndim
+    lst = [conv(x) for x in arg]
+    if len(lst) != ndim:
+        raise RuntimeError(f"{name} must have length equal to input rank")
+    return lst
+
+
+def check_axes(axes, ndim):
+    """UTIL:111-127."""
+    if axes is None:
+        return tuple(range(ndim))
+    if np.isscalar(axes):
+        axes = (int(axes),)
+    else:
+        axes = tuple(int(a) for a in axes)
+        for ax in axes:
+            if ax < -ndim or ax > ndim - 1:
+                raise np.exceptions.AxisError(f"specified axis: {ax} is out of range")
+        axes = tuple(a % ndim for a in axes)
+    if len(set(axes)) != len(axes):
+        raise ValueError("axes must be unique")
+    return axes
+
+
+# ------------------------------------------------------------- kernel choice
+
+def _smem_bytes(ndim, axis, K, anchor, itemsize):
+    """SEP:17-69 (_get_constants) and SEP:72-88 (_get_smem_shape)."""
+    hpn = max(K - anchor, anchor)
+    if ndim == 2:
+        bx, by, bz = (16, 16, 1) if axis == 1 else (32, 8, 1)
+        halo = math.ceil(hpn / (bx if axis == 1 else by))
+    else:
+        if axis == 2:
+            bx, by, bz = 16, 4, 4
+            halo = math.ceil(hpn / bx)
+        elif axis == 1:
+            bx, by, bz = 32, 4, 4
+            halo = math.ceil(hpn / by)
+        else:
+            bx, by, bz = 32, 4, 4
+            halo = math.ceil(hpn / bz)
+    ppb = max(4, halo)
+    return (ppb + 2 * halo) * bx * by * bz * itemsize
+
+
+def choose_path(ndim, axis, K, anchor, mode, cval, in_dtype, algorithm=None):
+    """FLT:271-344: 'shared_memory' or 'elementwise' for one correlate1d call."""
+    in_dtype = np.dtype(in_dtype)
+    default = algorithm is None
+    if default:
+        if ndim == 2 and K <= 256 and not (cval < 0 and mode == "constant" and in_dtype.kind == "u"):
+            algorithm = "shared_memory"
+        else:
+            algorithm = "elementwise"
+    elif algorithm == "shared_memory":
+        if mode == "constant" and (not np.isfinite(cval) or (cval < 0 and in_dtype.kind == "u")):
+            algorithm = "elementwise"
+    elif algorithm != "elementwise":
+        raise ValueError("algorithm must be 'shared_memory', 'elementwise' or None")
+    if algorithm == "shared_memory":
+        if ndim not in (2, 3):
+            raise NotImplementedError(f"shared_memory not implemented for ndim={ndim}")
+        # compile failure on a non-finite fill value (SEP:219-223) and the
+        # shared-memory size check (SEP:1007-1017) fall back to elementwise
+        if mode == "constant" and not np.isfinite(cval):
+            return "elementwise"
+        if K > 32 and _smem_bytes(ndim, axis, K, anchor, in_dtype.itemsize) > SHARED_BLOCK_BYTES:
+            return "elementwise"
+    return algorithm
+
+
+def pass_params(in_dtype, ndim, axis, weights, mode, cval, origin, convolve, algorithm=None):
+    """Everything the per-output arithmetic of one correlate1d call depends on.
+
+    Returns (taps_in_W (float64 array), anchor, mode_code, cval_w, w64, skip_zero).
+    """
+    weights = np.asarray(weights)
+    if weights.ndim != 1 or weights.size < 1:
+        raise RuntimeError("incorrect filter size")
+    K = weights.size
+    origin = check_origin(origin, K)
+    if mode == "wrap":
+        mode = "grid-wrap"
+    check_mode(mode)
+    if convolve:
+        weights = weights[::-1]
+        origin = -origin
+        if K % 2 == 0:
+            origin -= 1
+    anchor = K // 2 + origin
+    wdt = weights_dtype(in_dtype, weights.dtype)
+    w64 = wdt == np.float64
+    taps = weights.astype(wdt).astype(np.float64)
+    path = choose_path(ndim, axis, K, anchor, mode, cval, in_dtype, algorithm)
+    if path == "shared_memory":
+        cval_w = _lib.oracle_cval_as_input(float(cval), _dchar(in_dtype), int(w64))
+        skip_zero = False
+    else:
+        cval_w = float(cval) if w64 else float(np.float32(cval))
+        skip_zero = True
+    return taps, anchor, MODES[mode], cval_w, int(w64), int(skip_zero), path
+
+
+def get_output(output, input, shape=None):
+    """UTIL:49-71 (real dtypes only)."""
+    shape = input.shape if shape is None else shape
+    if output is None:
+        return np.empty(shape, dtype=input.dtype)
+    if isinstance(output, (type, np.dtype, str)):
+        return np.empty(shape, dtype=np.dtype(output))
+    if output.shape != shape:
+        raise RuntimeError("output shape not correct")
+    return output
+
+
+# --------------------------------------------------------------- 1-D passes
+
+def _run_pass(x, out, axis, taps, anchor, mode_code, cval_w, w64, skip_zero):
+    x = np.ascontiguousarray(x)
+    assert out.flags.c_contiguous and out.shape == x.shape
+    shape = x.shape
+    outer = int(np.prod(shape[:axis], dtype=np.int64))
+    L = shape[axis]
+    inner = int(np.prod(shape[axis + 1:], dtype=np.int64))
+    t = np.ascontiguousarray(taps, dtype=np.float64)
+    _lib.oracle_correlate1d(
+        x.ctypes.data, ord(x.dtype.char), out.ctypes.data, ord(out.dtype.char),
+        outer, L, inner, t.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), t.size,
+        anchor, mode_code, cval_w, w64, skip_zero, THREADS,
+    )
+    return out
+
+
+def correlate1d(input, weights, axis=-1, output=None, mode="reflect", cval=0.0,
+                origin=0, *, algorithm=None, convolve=False):
+    """FLT:135-178 / FLT:180-221 -> FLT:271-344."""
+    input = np.asarray(input)
+    axis = axis % input.ndim if input.ndim else 0
+    params = pass_params(input.dtype, input.ndim, axis, weights, mode, cval, origin,
+                         convolve, algorithm)
+    out = get_output(output, input)
+    if out.dtype.kind in "iu" and mode == "constant" and params[-1] == "elementwise" \
+            and not np.isfinite(cval):
+        raise NotImplementedError(
+            "Non-finite cval is not supported for outputs with integer dtype.")
+    res = np.empty(input.shape, out.dtype)
+    _run_pass(input, res, axis, *params[:-1])
+    out[...] = res
+    return out
+
+
+def convolve1d(input, weights, axis=-1, output=None, mode="reflect", cval=0.0,
+               origin=0, *, algorithm=None):
+    return correlate1d(input, weights, axis, output, mode, cval, origin,
+                       algorithm=algorithm, convolve=True)
+
+
+def run_1d_correlates(input, axes, weight_list, output, modes, cval, origins=0,
+                      algorithm=None, convolve=False):
+    """CORE:124-163 with FLT:363-396: passes in axis order, intermediates in
+    the output dtype, ping-pong between output and one temporary."""
+    input = np.asarray(input)
+    output = get_output(output, input)
+    axes = check_axes(axes, input.ndim)
+    n = len(axes)
+    modes = fix_sequence_arg(modes, n, "mode", check_mode)
+    modes = ["grid-wrap" if m == "wrap" else m for m in modes]
+    origins = fix_sequence_arg(origins, n, "origin", int)
+    work = [(ax, w, m, o) for ax, w, m, o in zip(axes, weight_list, modes, origins) if w is not None]
+    if not work:
+        output[...] = input
+        return output
+    cur = input
+    for ax, w, m, o in work:
+        res = np.empty(input.shape, output.dtype)
+        correlate1d(cur, w, ax, res, m, cval, o, algorithm=algorithm, convolve=convolve)
+        cur = res
+    output[...] = cur
+    return output
+
+
+# ------------------------------------------------------------- filter family
+
+def gaussian_kernel1d(sigma, order, radius, dtype=np.float64):
+    """FLT:689-717 (order 0 returns float64 regardless of `dtype`)."""
+    if order < 0:
+        raise ValueError("order must be non-negative")
+    sigma2 = sigma * sigma
+    x = np.arange(-radius, radius + 1)
+    phi_x = np.exp(-0.5 / sigma2 * x**2)
+    phi_x /= phi_x.sum()
+    if order == 0:
+        return phi_x
+    exponent_range = np.arange(order + 1)
+    q = np.zeros(order + 1)
+    q[0] = 1
+    D = np.diag(exponent_range[1:], 1)
+    P = np.diag(np.ones(order) / -sigma2, -1)
+    Q_deriv = D + P
+    for _ in range(order):
+        q = Q_deriv.dot(q)
+    q = (x[:, None] ** exponent_range).dot(q)
+    return np.ascontiguousarray((q * phi_x)[::-1], dtype=dtype)
+
+
+def gaussian_filter(input, sigma, order=0, output=None, mode="reflect", cval=0.0,
+                    truncate=4.0, radius=None, axes=None, *, algorithm=None):
+    """FLT:580-686."""
+    input = np.asarray(input)
+    axes = check_axes(axes, input.ndim)
+    n = len(axes)
+    sigmas = fix_sequence_arg(sigma, n, "sigma", float)
+    if n == 0 or all(s < 1e-15 for s in sigmas):
+        out = get_output(output, input)
+        out[...] = input
+        return out
+    orders = fix_sequence_arg(order, n, "order", int)
+    modes = fix_sequence_arg(mode, n, "mode", str)
+    radiuses = fix_sequence_arg(radius, n, "radius")
+    truncate = float(truncate)
+    wdt = np.promote_types(input.dtype, np.float32)
+    params = [(axes[i], sigmas[i], orders[i], modes[i], radiuses[i])
+              for i in range(n) if sigmas[i] > 1e-15]
+    ws = []
+    for _, s, o, _, r in params:
+        if r is None:
+            r = int(truncate * float(s) + 0.5)
+        ws.append(None if r <= 0 else gaussian_kernel1d(s, o, r, dtype=wdt))
+    return run_1d_correlates(input, [p[0] for p in params], ws, output,
+                             [p[3] for p in params], cval, 0, algorithm)
+
+
+def gaussian_filter1d(input, sigma, axis=-1, order=0, output=None, mode="reflect",
+                      cval=0.0, truncate=4.0, *, algorithm=None):
+    """FLT:524-577."""
+    input = np.asarray(input)
+    radius = int(float(truncate) * float(sigma) + 0.5)
+    wdt = np.promote_types(input.dtype, np.float32)
+    w = gaussian_kernel1d(sigma, int(order), radius, wdt)
+    return correlate1d(input, w, axis, output, mode, cval, algorithm=algorithm)
+
+
+def uniform_filter1d(input, size, axis=-1, output=None, mode="reflect", cval=0.0,
+                     origin=0, *, algorithm=None):
+    """FLT:399-444."""
+    input = np.asarray(input)
+    wdt = np.promote_types(input.dtype, np.float32)
+    w = np.full(size, 1 / size, dtype=wdt)
+    return correlate1d(input, w, axis, output, mode, cval, origin, algorithm=algorithm)
+
+
+def uniform_filter(input, size=3, output=None, mode="reflect", cval=0.0, origin=0,
+                   axes=None, *, algorithm=None):
+    """FLT:447-521."""
+    input = np.asarray(input)
+    axes = check_axes(axes, input.ndim)
+    n = len(axes)
+    sizes = fix_sequence_arg(size, n, "size", int)
+    origins = fix_sequence_arg(origin, n, "origin", int)
+    modes = fix_sequence_arg(mode, n, "mode", str)
+    wdt = np.promote_types(input.dtype, np.float32)
+    ws = [None if s <= 1 else np.full(s, 1 / s, dtype=wdt) for s in sizes]
+    return run_1d_correlates(input, axes, ws, output, modes, cval, origins, algorithm)
+
+
+def _prewitt_or_sobel(input, axis, output, mode, cval, smooth, algorithm):
+    """FLT:782-803."""
+    input = np.asarray(input)
+    axis = axis % input.ndim
+    wdt = np.promote_types(input.dtype, np.float32)
+    diff = np.array([-1, 0, 1], dtype=wdt)
+    ws = [diff if a == axis else smooth for a in range(input.ndim)]
+    return run_1d_correlates(input, tuple(range(input.ndim)), ws, output,
+                             (mode,) * input.ndim, cval, 0, algorithm)
+
+
+def sobel(input, axis=-1, output=None, mode="reflect", cval=0.0, *, algorithm=None):
+    """FLT:751-779."""
+    input = np.asarray(input)
+    wdt = np.promote_types(input.dtype, np.float32)
+    return _prewitt_or_sobel(input, axis, output, mode, cval,
+                             np.array([1, 2, 1], dtype=wdt), algorithm)
+
+
+def prewitt(input, axis=-1, output=None, mode="reflect", cval=0.0, *, algorithm=None):
+    """FLT:720-748."""
+    input = np.asarray(input)
+    wdt = np.promote_types(input.dtype, np.float32)
+    return _prewitt_or_sobel(input, axis, output, mode, cval,
+                             np.ones(3, dtype=wdt), algorithm)
+
+
+def gaussian_gradient_magnitude(input, sigma, output=None, mode="reflect", cval=0.0,
+                                *, axes=None, algorithm=None, **kwargs):
+    """FLT:1100-1157 over generic_gradient_magnitude FLT:1012-1097 (float outputs)."""
+    input = np.asarray(input)
+    ndim = input.ndim
+    axes = check_axes(axes, ndim)
+    modes = fix_sequence_arg(mode, len(axes), "mode", check_mode)
+    output = get_output(output, input)
+    if output.dtype.kind != "f":
+        raise NotImplementedError("integer output")
+
+    def deriv(ax, m):
+        order = [0] * ndim
+        order[ax] = 1
+        return gaussian_filter(input, sigma, order, output.dtype, m, cval,
+                               algorithm=algorithm, **kwargs)
+
+    acc = deriv(axes[0], modes[0])
+    acc = acc * acc
+    for i in range(1, len(axes)):
+        t = deriv(axes[i], modes[i])
+        acc = acc + t * t
+    output[...] = np.sqrt(acc)
+    return output
+
+
+# ---------------------------------------------------------- skimage layer
+
+def sk_gaussian(image, sigma=1, mode="nearest", cval=0, preserve_range=False,
+                truncate=4.0, *, channel_axis=None, out=None):
+    """_shared/filters.py:21-166."""
+    image = np.asarray(image)
+    if not np.iterable(sigma):
+        if sigma < 0:
+            raise ValueError("Sigma values less than zero are not valid")
+    elif any(s < 0 for s in sigma):
+        raise ValueError("Sigma values less than zero are not valid")
+    if channel_axis is not None:
+        axes = tuple(a for a in range(image.ndim) if a != channel_axis % image.ndim)
+    else:
+        axes = tuple(range(image.ndim))
+    image = convert_to_float(image, preserve_range)
+    image = image.astype(supported_float_type(image.dtype), copy=False)
+    res = gaussian_filter(image, sigma, output=image.dtype, mode=mode, cval=cval,
+                          truncate=truncate, axes=axes)
+    if out is not None:
+        out[...] = res
+        return out
+    return res
+
+
+_SOBEL_SMOOTH = np.array([1, 2, 1]) / 4
+_PREWITT_SMOOTH = np.full((3,), 1 / 3)
+
+
+def generic_edge_filter(image, *, smooth_weights, edge_weights=(1, 0, -1), axis=None,
+                        mode="reflect"):
+    """filters/edges.py:148-241 (cval is accepted there but never forwarded)."""
+    image = np.asarray(image)
+    ndim = image.ndim
+    if axis is None:
+        axes = list(range(ndim))
+    elif np.isscalar(axis):
+        axes = [axis]
+    else:
+        axes = list(axis)
+    mag = len(axes) > 1
+    if image.dtype.kind == "f":
+        fdt = supported_float_type(image.dtype)
+        image = image.astype(fdt, copy=False)
+    else:
+        image = img_as_float(image)
+        fdt = image.dtype
+    ew = np.asarray(edge_weights, dtype=fdt)
+    sw = np.asarray(smooth_weights, dtype=fdt)
+    if mag:
+        ew = (ew / fdt.type(math.sqrt(ndim))).astype(fdt)
+    output = None
+    for i, ed in enumerate(axes):
+        ax_out = convolve1d(image, ew, axis=ed, mode=mode, output=fdt)
+        for sd in sorted(set(range(ndim)) - {ed % ndim}):
+            ax_out = convolve1d(ax_out, sw, axis=sd, mode=mode, output=fdt)
+        if mag:
+            ax_out = (ax_out * ax_out).astype(fdt)
+        output = ax_out if i == 0 else (output + ax_out).astype(fdt)
+    if mag:
+        output = np.sqrt(output).astype(fdt)
+    return output
+
+
+def sk_sobel(image, mask=None, *, axis=None, mode="reflect", cval=0.0):
+    return generic_edge_filter(image, smooth_weights=_SOBEL_SMOOTH, axis=axis, mode=mode)
+
+
+def sk_prewitt(image, mask=None, *, axis=None, mode="reflect", cval=0.0):
+    return generic_edge_filter(image, smooth_weights=_PREWITT_SMOOTH, axis=axis, mode=mode)
+
+
+def hessian_matrix_gaussian(image, sigma=1, mode="reflect", cval=0, order="rc"):
+    """feature/corner.py:161-254 (use_gaussian_derivatives=True)."""
+    image = img_as_float(np.asarray(image))
+    image = image.astype(supported_float_type(image.dtype), copy=False)
+    ndim = image.ndim
+    if np.isscalar(sigma):
+        sigma = (sigma,) * ndim
+    truncate = 8 if all(s > 1 for s in sigma) else 100
+    sq1_2 = 1 / math.sqrt(2)
+    ss = tuple(sq1_2 * s for s in sigma)
+    orders = [tuple([0] * d + [1] + [0] * (ndim - d - 1)) for d in range(ndim)]
+    grads = [gaussian_filter(image, ss, order=orders[d], mode=mode, cval=cval,
+                             truncate=truncate) for d in range(ndim)]
+    axes = list(range(ndim))
+    if order == "xy":
+        axes = axes[::-1]
+    return [gaussian_filter(grads[a0], ss, order=orders[a1], mode=mode, cval=cval,
+                            truncate=truncate)
+            for a0, a1 in combinations_with_replacement(axes, 2)]
+
+
+def gradient(f, axis=None):
+    """numpy/cupy gradient with unit spacing and edge_order=1."""
+    f = np.asarray(f)
+    axes = range(f.ndim) if axis is None else [axis]
+    outs = []
+    for ax in axes:
+        out = np.empty_like(f)
+        sl = [slice(None)] * f.ndim
+
+        def S(s):
+            sl2 = list(sl)
+            sl2[ax] = s
+            return tuple(sl2)
+
+        out[S(slice(1, -1))] = (f[S(slice(2, None))] - f[S(slice(None, -2))]) / f.dtype.type(2.0)
+        out[S(0)] = f[S(1)] - f[S(0)]
+        out[S(-1)] = f[S(-1)] - f[S(-2)]
+        outs.append(out)
+    return outs if axis is None else outs[0]
+
+
+def hessian_matrix_fd(image, sigma=1, mode="constant", cval=0, order="rc"):
+    """feature/corner.py:355-384 (use_gaussian_derivatives=False)."""
+    image = img_as_float(np.asarray(image))
+    image = image.astype(supported_float_type(image.dtype), copy=False)
+    ch = -1 if (image.ndim == 3 and image.shape[-1] == 3) else None
+    g = sk_gaussian(image, sigma=sigma, mode=mode, cval=cval, channel_axis=ch)
+    grads = gradient(g)
+    axes = list(range(image.ndim))
+    if order == "xy":
+        axes = axes[::-1]
+    return [gradient(grads[a0], axis=a1) for a0, a1 in combinations_with_replacement(axes, 2)]
+
+
+def eigvals_sym(elems, sort="descending", abs_sort=False):
+    """feature/corner.py:699-755 with the closed forms of :473-527 and :566-647,
+    evaluated in float64 (the 3x3 kernel's own precision) and rounded to F."""
+    F = elems[0].dtype
+    e = [np.asarray(x, dtype=np.float64) for x in elems]
+    if len(e) == 3:
+        m00, m01, m11 = e
+        # the 2x2 kernel keeps its temporaries in F
+        t1 = (m01 * m01).astype(F) * F.type(4)
+        t2 = (m00 - m11).astype(F)
+        t2 = (t2 * t2 + t1).astype(F)
+        t2 = (np.sqrt(t2) / F.type(2)).astype(F)
+        t1 = ((m00 + m11).astype(F) / F.type(2)).astype(F)
+        lo, hi = (t1 - t2).astype(F), (t1 + t2).astype(F)
+        l1, l2 = (lo, hi) if sort == "ascending" else (hi, lo)
+        if abs_sort:
+            sw = (np.abs(l1) > np.abs(l2)) if sort == "ascending" else (np.abs(l1) < np.abs(l2))
+            l1, l2 = np.where(sw, l2, l1), np.where(sw, l1, l2)
+        return np.stack([l1, l2])
+    else:
+        a, d, f, b, ee, c = e
+        d_sq, e_sq, f_sq = d * d, ee * ee, f * f
+        ta, tb, tc = 2 * a - b - c, 2 * b - a - c, 2 * c - a - b
+        x2 = -ta * tb * tc + 9 * (tc * d_sq + tb * f_sq + ta * e_sq) - 54 * (d * ee * f)
+        x1 = a * a + b * b + c * c - a * b - a * c - b * c + 3 * (d_sq + e_sq + f_sq)
+        x1 = np.maximum(x1, 0.0)
+        arg = np.maximum(4 * x1 ** 3 - x2 ** 2, 0.0)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            phi = np.arctan(np.sqrt(arg) / x2)
+        phi = np.where(x2 < 0, phi + np.pi, phi)
+        phi = np.where(x2 == 0.0, np.pi / 2.0, phi)
+        x1t = (2.0 / 3.0) * np.sqrt(x1)
+        abc = (a + b + c) / 3.0
+        lam = [(abc - x1t * np.cos(phi / 3.0)).astype(F),
+               (abc + x1t * np.cos((phi - np.pi) / 3.0)).astype(F),
+               (abc + x1t * np.cos((phi + np.pi) / 3.0)).astype(F)]
+        # The three compare-and-swap steps of corner.py:607-629. With
+        # abs_sort the magnitudes are taken once, before any swap, and the
+        # comparisons keep using those original magnitudes.
+        keys = [np.abs(v) for v in lam] if abs_sort else None
+        order = (0, 1, 2) if sort == "ascending" else (2, 1, 0)
+        v1, v2, v3 = order
+
+        def step(i, j):
+            ki = keys[i] if abs_sort else lam[i]
+            kj = keys[j] if abs_sort else lam[j]
+            sw = ki > kj
+            lam[i], lam[j] = np.where(sw, lam[j], lam[i]), np.where(sw, lam[i], lam[j])
+
+        step(v1, v2)
+        step(v1, v3)
+        step(v2, v3)
+        return np.stack(lam)
+
+
+def frangi(image, sigmas=range(1, 10, 2), alpha=0.5, beta=0.5, gamma=None,
+           black_ridges=True, mode="reflect", cval=0):
+    """filters/ridges.py:322-476 with the kernels of :228-319."""
+    image = np.asarray(image)
+    image = image.astype(supported_float_type(image.dtype), copy=False)
+    if not black_ridges:
+        image = -image
+    F = image.dtype
+    alpha_sq, beta_sq = 2 * alpha * alpha, 2 * beta * beta
+    gamma_sq = None if gamma is None else 2 * gamma * gamma
+    fmax = None
+    for sigma in sigmas:
+        H = hessian_matrix_gaussian(image, sigma, mode=mode, cval=cval)
+        ev = eigvals_sym(H, sort="ascending", abs_sort=True)
+        rg = np.zeros(image.shape, F)
+        for lam in ev:
+            rg = (rg + lam.astype(np.float64) * lam).astype(F)
+        if gamma_sq is None:
+            s_max = float(rg.max())
+            g = math.sqrt(s_max) / 2.0
+            gamma_sq = 2.0 if s_max == 0 else max(2 * g * g, 1e-10)
+        if image.ndim == 2:
+            l1, l2 = ev
+            rb = (np.abs(l1) / np.maximum(l2, F.type(1e-10))).astype(F)
+            rb = (rb * rb).astype(F)
+            v = np.exp(-rb.astype(np.float64) / beta_sq).astype(F)
+            v = (v * (1.0 - np.exp(-rg.astype(np.float64) / gamma_sq))).astype(F)
+        else:
+            l1, l2, l3 = ev
+            lam2 = np.maximum(l2, F.type(1e-10))
+            lam3 = np.maximum(l3, F.type(1e-10))
+            ra = (lam2 / lam3).astype(F)
+            ra = (ra * ra).astype(F)
+            rb = ((l1 * l1).astype(F) / (lam2 * lam3).astype(F)).astype(F)
+            v = (1.0 - np.exp(-ra.astype(np.float64) / alpha_sq)).astype(F)
+            v = (v * np.exp(-rb.astype(np.float64) / beta_sq)).astype(F)
+            v = (v * (1.0 - np.exp(-rg.astype(np.float64) / gamma_sq))).astype(F)
+        fmax = v.copy() if fmax is None else np.maximum(fmax, v)
+    return fmax
+
+
+def rgb2gray(rgb, channel_axis=-1):
+    """color/colorconv.py:1049-1095 (+ _prepare_colorarray :160-183)."""
+    rgb = np.moveaxis(np.asarray(rgb), channel_axis, -1)
+    if rgb.shape[-1] != 3:
+        raise ValueError("the input array must have size 3 along `channel_axis`")
+    fdt = supported_float_type(rgb.dtype)
+    x = img_as_float(rgb).astype(fdt)
+    x = np.ascontiguousarray(x).astype(np.float64)
+    g = 0.2125 * x[..., 0] + 0.7154 * x[..., 1] + 0.0721 * x[..., 2]
+    return g.astype(fdt)
+
+
+def cast_w(values_w, w64, out_dtype):
+    """cast<D>() of a W-typed array alone (CORE:227-244)."""
+    src = np.ascontiguousarray(values_w, dtype=np.float64 if w64 else np.float32)
+    out = np.empty(src.shape, dtype=out_dtype)
+    _lib.oracle_cast(src.ctypes.data, int(w64), out.ctypes.data, ord(out.dtype.char), src.size)
+    return out

@@ -1,0 +1,120 @@
+"""libcimx.so without a GPU: it loads, exports every entry point that
+include/cimx.h declares, rejects bad arguments before touching the device,
+and the Python host logic agrees with the oracle's restatement."""
+
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from cucim_b200 import _lib, _util
+from cucim_b200 import ndimage as ndi
+from oracle import restate as R
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared():
+    text = open(os.path.join(ROOT, "include", "cimx.h")).read()
+    return re.findall(r"CIMX_API\s+[\w\s\*]+?\b(cimx_\w+)\s*\(", text)
+
+
+def test_every_declared_symbol_is_exported():
+    names = _declared()
+    assert len(names) >= 10
+    for n in names:
+        assert hasattr(_lib.lib, n), n
+        assert n in _lib.EXPORTED, f"{n} has no ctypes signature"
+
+
+def test_abi_version():
+    assert _lib.lib.cimx_abi_version() == 100
+
+
+def _arr(shape, dtype, ptr=0x1000, strides=None):
+    a = _lib.CimxArray()
+    a.data = ptr
+    a.dtype = ord(np.dtype(dtype).char)
+    a.ndim = len(shape)
+    es = np.dtype(dtype).itemsize
+    if strides is None:
+        strides, acc = [], es
+        for n in reversed(shape):
+            strides.insert(0, acc)
+            acc *= n
+    for d, (n, s) in enumerate(zip(shape, strides)):
+        a.shape[d] = n
+        a.strides[d] = s
+    return a
+
+
+def _corr(a_in, a_out, K=3, axis=0, origin=0, mode=0):
+    t, p = _lib.taps_pointer(np.ones(K))
+    return _lib.lib.cimx_correlate1d(ctypes.byref(a_in), ctypes.byref(a_out), p, K, axis,
+                                     origin, mode, 0.0, 0, None)
+
+
+def test_validation_happens_before_device_work():
+    good_in = _arr((4, 5), np.float32, 0x1000)
+    good_out = _arr((4, 5), np.float32, 0x9000)
+    assert _corr(good_in, _arr((4, 6), np.float32, 0x9000)) == _lib.E_INVALID
+    assert "shape" in _lib.last_error()
+    assert _corr(good_in, _arr((4, 5), np.complex64, 0x9000)) == _lib.E_DTYPE
+    assert _corr(_arr((4, 5), np.float32, 0x1000, strides=(4, 16)), good_out) == _lib.E_LAYOUT
+    assert _corr(good_in, good_out, K=3, origin=2) == _lib.E_INVALID
+    assert "origin" in _lib.last_error()
+    assert _corr(good_in, good_out, mode=9) == _lib.E_INVALID
+    assert _corr(good_in, good_out, axis=2) == _lib.E_INVALID
+    assert _corr(good_in, _arr((4, 5), np.float32, 0x1004)) == _lib.E_INVALID  # overlap
+    assert _corr(good_in, good_out, K=0) == _lib.E_INVALID
+
+
+def test_check_maps_errors_like_cucim():
+    with pytest.raises(MemoryError):
+        _lib.check(_lib.E_NOMEM, "x")
+    with pytest.raises(RuntimeError):
+        _lib.check(_lib.E_CUDA, "x")
+
+
+@pytest.mark.parametrize("ndim", [2, 3])
+@pytest.mark.parametrize("K", [3, 33, 200, 257])
+@pytest.mark.parametrize("dtype", [np.uint8, np.uint16, np.float32, np.float64])
+@pytest.mark.parametrize("mode,cval", [("reflect", 0.0), ("constant", -1.0),
+                                       ("constant", np.nan), ("constant", 2.0)])
+def test_algorithm_choice_matches_oracle(ndim, K, dtype, mode, cval):
+    for axis in range(ndim):
+        anchor = K // 2
+        assert _util.choose_algorithm(ndim, axis, K, anchor, mode, cval, dtype) == \
+            R.choose_path(ndim, axis, K, anchor, mode, cval, dtype)
+
+
+@pytest.mark.parametrize("sigma", [0.5, 1.0, 0.7071067811865476, 3.3, 16.0, 32.0])
+@pytest.mark.parametrize("order", [0, 1, 2])
+def test_gaussian_taps_match_oracle(sigma, order):
+    r = int(4.0 * sigma + 0.5)
+    a = ndi._gaussian_kernel1d(sigma, order, r, np.float32)
+    b = R.gaussian_kernel1d(sigma, order, r, np.float32)
+    assert a.dtype == b.dtype
+    np.testing.assert_array_equal(a, b)
+
+
+def test_pass_flags():
+    f = _util.pass_flags(np.uint16, 3, 0, 9, 0, "mirror", 0.0, np.float64, False, None)
+    assert f & _lib.F_SKIP_ZERO_TAPS and not f & _lib.F_W64
+    f = _util.pass_flags(np.float64, 2, 0, 9, 0, "mirror", 0.0, np.float64, True, None)
+    assert f & _lib.F_CVAL_AS_INPUT and f & _lib.F_W64 and f & _lib.F_CONVOLVE
+    f = _util.pass_flags(np.int32, 2, 1, 5, 0, "reflect", 0.0, np.float32, False, None)
+    assert f & _lib.F_W64  # promote(int32, float32) = float64
+
+
+def test_modes_and_axes_checks():
+    with pytest.raises(RuntimeError):
+        _util.check_mode("grid-reflect")
+    with pytest.raises(RuntimeError):
+        _util.check_mode("bogus")
+    with pytest.raises(ValueError):
+        _util.check_axes((0, 0), 2)
+    assert _util.check_axes(-1, 3) == (-1,)  # scalars are not normalised (UTIL:114-115)
+    assert _util.check_axes([-1], 3) == (2,)
