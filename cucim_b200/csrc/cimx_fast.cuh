@@ -1,0 +1,565 @@
+// cimx_fast.cuh — kernel templates of the plain (exact float32) fast path.
+//
+// (a) k_stream: one pass along a strided axis of the view (outer, L, inner).
+//     Each thread owns 4 consecutive inner positions (one 4-wide vector
+//     load/store per row) and walks a chunk of L. The last K rows, plus PF
+//     rows prefetched ahead, live in a register ring indexed at compile time:
+//     every input row is read once per chunk, loads are issued PF rows before
+//     they are used, and every tap is a constant-bank FMA operand.
+// (b) k_slab: the last two axes (y, x) of a (B, Y, X) view in one launch. One
+//     TMA bulk tensor copy brings the halo'd input tile into shared memory
+//     (zero-filled outside the array); tiles touching the border get their
+//     halo rewritten with the boundary mode's values. The y pass writes its
+//     result, rounded through the output dtype as cuCIM's ping-pong does, to a
+//     second shared tile and the x pass stores the outputs: the intermediate
+//     never reaches HBM.
+//
+// Every output is the same fused multiply-add chain as in the generic
+// kernels (taps ascending, float32 FMA from +0, cast<D>()), so a pass list
+// gives bit-identical results whichever kernels run it.
+#pragma once
+
+#include <algorithm>
+#include <cstring>
+#include <mutex>
+
+#include "cimx_common.cuh"
+#include "cimx_fused.h"
+#include "cimx_tma.cuh"
+
+namespace cimx {
+namespace fast {
+
+constexpr int P = 8;  // consecutive outputs per thread in the slab kernel
+constexpr int kMaxSmem = 227 * 1024;
+
+// ------------------------------------------------------------ vector I/O
+
+template <class T> struct Vec4;
+template <> struct Vec4<float> { using type = float4; };
+template <> struct Vec4<uint16_t> { using type = ushort4; };
+template <> struct Vec4<uint8_t> { using type = uchar4; };
+
+template <class T>
+__device__ __forceinline__ void load4(const T* p, float (&v)[4]) {
+  const typename Vec4<T>::type q = *reinterpret_cast<const typename Vec4<T>::type*>(p);
+  v[0] = static_cast<float>(q.x);
+  v[1] = static_cast<float>(q.y);
+  v[2] = static_cast<float>(q.z);
+  v[3] = static_cast<float>(q.w);
+}
+
+template <class D>
+__device__ __forceinline__ void store4(D* p, float a, float b, float c, float d) {
+  typename Vec4<D>::type q;
+  q.x = out_cast<D>(a);
+  q.y = out_cast<D>(b);
+  q.z = out_cast<D>(c);
+  q.w = out_cast<D>(d);
+  *reinterpret_cast<typename Vec4<D>::type*>(p) = q;
+}
+
+template <class T> constexpr int dt_code();
+template <> constexpr int dt_code<float>() { return DT_F32; }
+template <> constexpr int dt_code<uint16_t>() { return DT_U16; }
+template <> constexpr int dt_code<uint8_t>() { return DT_U8; }
+
+// ------------------------------------------------------------- helpers
+
+// Two independent IEEE float32 FMAs (round to nearest) in one instruction:
+// d.x = fma(a.x, b.x, c.x), d.y = fma(a.y, b.y, c.y), bit-identical to fmaf.
+__device__ __forceinline__ float2 ffma2(float2 a, float2 b, float2 c) {
+  float2 d;
+  asm("{.reg .b64 ra, rb, rc, rd;\n"
+      " mov.b64 ra, {%2, %3};\n mov.b64 rb, {%4, %5};\n mov.b64 rc, {%6, %7};\n"
+      " fma.rn.f32x2 rd, ra, rb, rc;\n"
+      " mov.b64 {%0, %1}, rd;\n}"
+      : "=f"(d.x), "=f"(d.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
+  return d;
+}
+
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_addr(dst)), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(dst)), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(smem_addr(dst)), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+template <class T>
+__device__ __forceinline__ void cp_async_vec4(T* dst, const T* src) {
+  if constexpr (sizeof(T) == 4) cp_async16(dst, src);
+  else if constexpr (sizeof(T) == 2) cp_async8(dst, src);
+  else cp_async4(dst, src);
+}
+
+// ---------------------------------------------------------------- (a)
+
+template <int K>
+struct StreamArgs {
+  const void* in;
+  void* out;
+  long long outer, L, inner;  // elements
+  long long nchunks, chunk;
+  int anchor, mode;
+  double cval;
+  int cval_as_input;
+  unsigned long long active;  // bit k set: tap k takes part in the chain
+  float w[K];
+};
+
+// rows in flight per thread: a multiple of K with at least 8 rows
+template <int K> constexpr int stream_depth() { return K * ((8 + K - 1) / K); }
+template <class T, int K> constexpr int stream_smem() {
+  return stream_depth<K>() * 256 * 4 * (int)sizeof(T);
+}
+
+template <class T, class D, int K, bool MASK>
+__global__ void __launch_bounds__(256) k_stream(const StreamArgs<K> a) {
+  constexpr int DEPTH = stream_depth<K>();
+  extern __shared__ __align__(16) unsigned char sm_stream[];
+  // this thread's prefetch slots: slot d at pre + d * 256 * 4
+  T* pre = reinterpret_cast<T*>(sm_stream) + threadIdx.x * 4;
+  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long i4n = a.inner >> 2;
+  const long long i4 = tid % i4n;
+  const long long rest = tid / i4n;
+  const long long c = rest % a.nchunks;
+  const long long o = rest / a.nchunks;
+  if (o >= a.outer) return;  // no barrier in this kernel
+  const long long l0 = c * a.chunk;
+  const long long l1 = min(l0 + a.chunk, a.L);
+  const T* in = static_cast<const T*>(a.in) + (o * a.L) * a.inner + i4 * 4;
+  D* out = static_cast<D*>(a.out) + (o * a.L) * a.inner + i4 * 4;
+  const float cv = fill_value<float>(a.cval, a.cval_as_input, dt_code<T>());
+
+  auto mapped = [&](long long coord) -> long long {
+    return (coord < 0 || coord >= a.L) ? map_coord(coord, a.L, a.mode) : coord;
+  };
+  auto load_row = [&](float (&v)[4], long long coord) {
+    const long long m = mapped(coord);
+    if (m < 0) {
+      v[0] = v[1] = v[2] = v[3] = cv;
+    } else {
+      load4<T>(in + m * a.inner, v);
+    }
+  };
+  // input row consumed at step s (output l0 + s): the newest row of its window
+  auto row_of_step = [&](long long s) { return l0 + s - a.anchor + K - 1; };
+  auto issue = [&](int slot, long long s) {
+    const long long m = mapped(row_of_step(s));
+    if (m >= 0) cp_async_vec4<T>(pre + slot * 1024, in + m * a.inner);
+    cp_commit();
+  };
+
+  // window ring: slot j holds input row (l0 - anchor + j) modulo K. Prefetch
+  // slot d holds the row consumed at step d modulo DEPTH; the slot refilled at
+  // step s is the one consumed at step s - 1, so no copy can land on a slot
+  // whose shared load is still in flight.
+  float win[K][4];
+#pragma unroll
+  for (int k = 0; k < K - 1; ++k) load_row(win[k], l0 - a.anchor + k);
+#pragma unroll
+  for (int d = 0; d < DEPTH - 1; ++d) issue(d, d);
+
+  const long long n = l1 - l0;
+  for (long long s0 = 0; s0 < n; s0 += DEPTH) {
+#pragma unroll
+    for (int u = 0; u < DEPTH; ++u) {
+      const long long s = s0 + u;
+      if (s < n) {
+        issue((u + DEPTH - 1) % DEPTH, s + DEPTH - 1);
+        cp_wait<DEPTH - 1>();
+        float* v = win[(u + K - 1) % K];
+        const long long m = mapped(row_of_step(s));
+        if (m < 0) {
+          v[0] = v[1] = v[2] = v[3] = cv;
+        } else {
+          const typename Vec4<T>::type q =
+              *reinterpret_cast<const typename Vec4<T>::type*>(pre + u * 1024);
+          v[0] = static_cast<float>(q.x);
+          v[1] = static_cast<float>(q.y);
+          v[2] = static_cast<float>(q.z);
+          v[3] = static_cast<float>(q.w);
+        }
+        float acc[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+          if (!MASK || ((a.active >> k) & 1ull)) {
+#pragma unroll
+            for (int e = 0; e < 4; ++e) acc[e] = fmaf(win[(u + k) % K][e], a.w[k], acc[e]);
+          }
+        }
+        store4<D>(out + (l0 + s) * a.inner, acc[0], acc[1], acc[2], acc[3]);
+      }
+    }
+  }
+  cp_wait<0>();
+}
+
+template <class T, class D, int K>
+int launch_stream_k(const PassDesc& d, const float* w, int anchor, bool interior_zero,
+                    const void* in, void* out, cudaStream_t st) {
+  StreamArgs<K> a{};
+  a.in = in;
+  a.out = out;
+  a.outer = d.outer;
+  a.L = d.L;
+  a.inner = d.inner;
+  a.anchor = anchor;
+  a.mode = d.mode;
+  a.cval = d.cval;
+  a.cval_as_input = d.cval_as_input ? 1 : 0;
+  a.active = 0;
+  for (int k = 0; k < K; ++k) {
+    a.w[k] = w[k];
+    if (!(d.skip_zero && w[k] == 0.f)) a.active |= 1ull << k;
+  }
+  static std::once_flag once;
+  std::call_once(once, [] {
+    cudaFuncSetAttribute(k_stream<T, D, K, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         kMaxSmem);
+    cudaFuncSetAttribute(k_stream<T, D, K, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         kMaxSmem);
+  });
+  // chunk of L per thread: small enough to fill the GPU a few times over
+  const long long lanes = d.outer * (d.inner / 4);
+  long long chunk = 64;
+  while (chunk > 8 && lanes * ((d.L + chunk - 1) / chunk) < 148LL * 2048 * 2) chunk /= 2;
+  a.chunk = chunk;
+  a.nchunks = (d.L + chunk - 1) / chunk;
+  const long long threads = lanes * a.nchunks;
+  const unsigned blocks = (unsigned)((threads + 255) / 256);
+  constexpr int smem = stream_smem<T, K>();
+  if (interior_zero)
+    k_stream<T, D, K, true><<<blocks, 256, smem, st>>>(a);
+  else
+    k_stream<T, D, K, false><<<blocks, 256, smem, st>>>(a);
+  return cuda_fail(cudaGetLastError(), "stream pass launch");
+}
+
+template <class T, class D>
+int launch_stream_td(const PassDesc& d, const float* w, int K, int anchor, bool interior_zero,
+                     const void* in, void* out, cudaStream_t st) {
+  switch (K) {
+    case 3: return launch_stream_k<T, D, 3>(d, w, anchor, interior_zero, in, out, st);
+    case 5: return launch_stream_k<T, D, 5>(d, w, anchor, interior_zero, in, out, st);
+    case 7: return launch_stream_k<T, D, 7>(d, w, anchor, interior_zero, in, out, st);
+    case 9: return launch_stream_k<T, D, 9>(d, w, anchor, interior_zero, in, out, st);
+    case 13: return launch_stream_k<T, D, 13>(d, w, anchor, interior_zero, in, out, st);
+    case 17: return launch_stream_k<T, D, 17>(d, w, anchor, interior_zero, in, out, st);
+    default: return CIMX_FUSED_DECLINED;
+  }
+}
+
+// ---------------------------------------------------------------- (b)
+
+constexpr int kSlabTY = 32;    // output rows per tile
+constexpr int kSlabTX = 128;   // output columns per tile
+
+__host__ __device__ constexpr int pad8(int c) { return c + (c >> 3); }
+
+// Compile-time tile geometry for taps bucket KB (both passes have K8 <= KB).
+// Shared memory: mbarrier | y taps | x taps (float2 pairs (t, t)) |
+// s_in (float, dense, RY x RX) | union { TMA tile (T, BY x BX),
+// s_mid (float2 row pairs, TY/2 x RXQ, columns at pad8(c)) }.
+template <class T, int KB>
+struct Geom {
+  static constexpr int RY = kSlabTY + KB;         // staged rows
+  static constexpr int RX = kSlabTX + KB;         // staged columns (even)
+  static constexpr int RXQ = pad8(RX) + 1;        // float2 row-pair stride of s_mid
+  static constexpr int VE = 16 / (int)sizeof(T);  // elements per 16 bytes
+  static constexpr int BX = (RX + VE - 1 + VE - 1) / VE * VE;  // TMA box width
+  static constexpr int BY = RY;                   // TMA box height
+  static constexpr int RAW = BX * BY * (int)sizeof(T);
+  static constexpr int MID = (kSlabTY / 2) * RXQ * 8;
+  static constexpr int OFF_W = 128;
+  static constexpr int OFF_IN = OFF_W + 2 * kSlabMaxK * 8;
+  static constexpr int SZ_IN = RY * RX * 4;
+  static constexpr int OFF_U = (OFF_IN + SZ_IN + 127) / 128 * 128;
+  static constexpr int SZ_U = RAW > MID ? RAW : MID;
+  static constexpr int SMEM = OFF_U + SZ_U;
+  static_assert(SZ_IN >= MID, "s_mid must fit in s_in's space");
+};
+
+__device__ __forceinline__ long long floor_div(long long a, long long b) {
+  return a >= 0 ? a / b : -((-a + b - 1) / b);
+}
+
+// One fused multiply-add chain per lane pair for P outputs: acc[p] +=
+// x[p + k] * w[k], k ascending. `at(q)` returns the staged input pair at
+// window offset q. Full chunks of P taps run without guards, two chunks per
+// iteration so that the window halves swap roles without register moves.
+template <class At>
+__device__ __forceinline__ void chain2(float2 (&acc)[P], const float2* w2, int K, int skip,
+                                       At at) {
+  float2 win[2 * P];
+#pragma unroll
+  for (int j = 0; j < P; ++j) win[j] = at(j);
+  int k0 = 0;
+  if (!skip) {
+    for (; k0 + 2 * P <= K; k0 += 2 * P) {
+#pragma unroll
+      for (int j = 0; j < P; ++j) win[P + j] = at(k0 + P + j);
+#pragma unroll
+      for (int j = 0; j < P; ++j) {
+        const float2 t = w2[k0 + j];
+#pragma unroll
+        for (int p = 0; p < P; ++p) acc[p] = ffma2(win[p + j], t, acc[p]);
+      }
+#pragma unroll
+      for (int j = 0; j < P; ++j) win[j] = at(k0 + 2 * P + j);
+#pragma unroll
+      for (int j = 0; j < P; ++j) {
+        const float2 t = w2[k0 + P + j];
+#pragma unroll
+        for (int p = 0; p < P; ++p) acc[p] = ffma2(win[(P + p + j) % (2 * P)], t, acc[p]);
+      }
+    }
+  }
+  for (; k0 < K; k0 += P) {
+#pragma unroll
+    for (int j = 0; j < P; ++j) win[P + j] = at(k0 + P + j);
+#pragma unroll
+    for (int j = 0; j < P; ++j) {
+      const float2 t = w2[k0 + j];
+      if (k0 + j < K && (!skip || t.x != 0.f)) {
+#pragma unroll
+        for (int p = 0; p < P; ++p) acc[p] = ffma2(win[p + j], t, acc[p]);
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < P; ++j) win[j] = win[P + j];
+  }
+}
+
+// Value of the staged element (gy, gx) of the slab, boundary modes applied.
+template <class T>
+__device__ __forceinline__ float staged_value(const T* in, long long gy, long long gx,
+                                              const SlabArgs& a, int my, int mx, float cy,
+                                              float cx) {
+  long long yy = gy, xx = gx;
+  if (gy < 0 || gy >= a.Y) yy = map_coord(gy, a.Y, my);
+  if (gx < 0 || gx >= a.X) xx = map_coord(gx, a.X, mx);
+  if (yy < 0) return cy;
+  if (xx < 0) return 0.f;  // x-constant columns are replaced after the y pass
+  return static_cast<float>(in[yy * a.X + xx]);
+}
+
+template <class T, class D, int KB, bool TMA>
+__global__ void __launch_bounds__(256) k_slab(const __grid_constant__ CUtensorMap map,
+                                               const SlabArgs a) {
+  using G = Geom<T, KB>;
+  extern __shared__ __align__(128) unsigned char smem[];
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem);
+  float2* wy = reinterpret_cast<float2*>(smem + G::OFF_W);
+  float2* wx = wy + kSlabMaxK;
+  float* s_in = reinterpret_cast<float*>(smem + G::OFF_IN);
+  T* raw = reinterpret_cast<T*>(smem + G::OFF_U);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+
+  long long bid = blockIdx.x;
+  const long long tx = bid % a.tiles_x;
+  bid /= a.tiles_x;
+  const long long ty = bid % a.tiles_y;
+  const long long b = bid / a.tiles_y;
+  const long long y0 = ty * kSlabTY, x0 = tx * kSlabTX;
+  const int ay = a.py.anchor;
+  const int ax = a.has_x ? a.px.anchor : 0;
+  const long long ys = y0 - ay, xst = x0 - ax;
+  const T* in = static_cast<const T*>(a.in) + b * a.Y * a.X;
+  D* out = static_cast<D*>(a.out) + b * a.Y * a.X;
+  const int my = a.py.mode;
+  const int mx = a.has_x ? a.px.mode : CIMX_MODE_NEAREST;
+  const float cy = fill_value<float>(a.py.cval, a.py.cval_as_input, a.py.dt);
+  const float cx = a.has_x ? fill_value<float>(a.px.cval, a.px.cval_as_input, a.px.dt) : 0.f;
+
+  // a tile whose staged region lies inside the array needs no boundary work
+  const bool interior = ys >= 0 && ys + G::RY <= a.Y && xst >= 0 && xst + G::RX <= a.X;
+  const long long xs = floor_div(xst, G::VE) * G::VE;  // 16-byte aligned TMA start column
+  const int off = static_cast<int>(xst - xs);
+
+  if (TMA && threadIdx.x == 0) {
+    mbar_init(bar, 1);
+    mbar_fence_init();
+  }
+  for (int k = threadIdx.x; k < kSlabMaxK; k += blockDim.x) {
+    const float ty_ = k < a.py.K ? a.py.w[k] : 0.f;
+    const float tx_ = (a.has_x && k < a.px.K) ? a.px.w[k] : 0.f;
+    wy[k] = make_float2(ty_, ty_);
+    wx[k] = make_float2(tx_, tx_);
+  }
+  __syncthreads();
+
+  // 1. stage the tile
+  bool from_raw = false;  // the y pass reads the TMA tile directly
+  if (TMA) {
+    if (threadIdx.x == 0) {
+      mbar_expect_tx(bar, G::RAW);
+      tma_load_3d(raw, &map, bar, static_cast<int>(xs), static_cast<int>(ys),
+                  static_cast<int>(b));
+    }
+    if (!mbar_wait(bar, 0, a.status)) return;
+    from_raw = interior;
+    if (!from_raw) {
+      // convert to float and apply the boundary modes
+      for (int r = warp; r < G::RY; r += 8) {
+        const long long gy = ys + r;
+        const bool yin = gy >= 0 && gy < a.Y;
+        for (int c = lane; c < G::RX; c += 32) {
+          const long long gx = xst + c;
+          float v;
+          if (yin && gx >= 0 && gx < a.X) v = static_cast<float>(raw[r * G::BX + off + c]);
+          else v = staged_value<T>(in, gy, gx, a, my, mx, cy, cx);
+          s_in[r * G::RX + c] = v;
+        }
+      }
+    }
+  } else {
+    for (int r = warp; r < G::RY; r += 8) {
+      const long long gy = ys + r;
+      for (int c = lane; c < G::RX; c += 32)
+        s_in[r * G::RX + c] = staged_value<T>(in, gy, xst + c, a, my, mx, cy, cx);
+    }
+  }
+  __syncthreads();
+
+  // the y result goes where nothing is read any more: s_in's space when the
+  // y pass reads the TMA tile, the TMA tile's space otherwise
+  float2* s_mid = reinterpret_cast<float2*>(from_raw ? smem + G::OFF_IN : smem + G::OFF_U);
+
+  // 2. y pass: one column pair x P rows per item
+  {
+    constexpr int pairs = G::RX / 2;
+    constexpr int groups = kSlabTY / P;
+    for (int item = threadIdx.x; item < pairs * groups; item += blockDim.x) {
+      const int c = 2 * (item % pairs);
+      const int rg = (item / pairs) * P;
+      float2 acc[P];
+#pragma unroll
+      for (int p = 0; p < P; ++p) acc[p] = make_float2(0.f, 0.f);
+      if (from_raw) {
+        const T* col = raw + rg * G::BX + off + c;
+        chain2(acc, wy, a.py.K, a.py.skip, [&](int q) {
+          return make_float2(static_cast<float>(col[q * G::BX]),
+                             static_cast<float>(col[q * G::BX + 1]));
+        });
+      } else {
+        const float2* col = reinterpret_cast<const float2*>(s_in + rg * G::RX + c);
+        chain2(acc, wy, a.py.K, a.py.skip, [&](int q) { return col[q * (G::RX / 2)]; });
+      }
+      if (a.has_x) {
+        const long long gx = xst + c;
+        const bool f0 = mx == CIMX_MODE_CONSTANT && (gx < 0 || gx >= a.X);
+        const bool f1 = mx == CIMX_MODE_CONSTANT && (gx + 1 < 0 || gx + 1 >= a.X);
+        float2* d0 = s_mid + (rg / 2) * G::RXQ + pad8(c);
+        float2* d1 = s_mid + (rg / 2) * G::RXQ + pad8(c + 1);
+#pragma unroll
+        for (int p = 0; p < P; p += 2) {
+          const float a0 = f0 ? cx : static_cast<float>(out_cast<D>(acc[p].x));
+          const float b0 = f0 ? cx : static_cast<float>(out_cast<D>(acc[p + 1].x));
+          const float a1 = f1 ? cx : static_cast<float>(out_cast<D>(acc[p].y));
+          const float b1 = f1 ? cx : static_cast<float>(out_cast<D>(acc[p + 1].y));
+          d0[(p / 2) * G::RXQ] = make_float2(a0, b0);
+          d1[(p / 2) * G::RXQ] = make_float2(a1, b1);
+        }
+      } else if (c < kSlabTX) {
+        // y only: store straight to the output
+#pragma unroll
+        for (int p = 0; p < P; ++p) {
+          const long long yy = y0 + rg + p;
+          if (yy < a.Y) {
+            if (x0 + c < a.X) out[yy * a.X + x0 + c] = out_cast<D>(acc[p].x);
+            if (x0 + c + 1 < a.X) out[yy * a.X + x0 + c + 1] = out_cast<D>(acc[p].y);
+          }
+        }
+      }
+    }
+  }
+
+  if (a.has_x) {
+    __syncthreads();
+    // 3. x pass: one row pair x P consecutive outputs per item
+    constexpr int gpr = kSlabTX / P;
+    for (int item = threadIdx.x; item < (kSlabTY / 2) * gpr; item += blockDim.x) {
+      const int rp = item / gpr;
+      const int g = (item % gpr) * P;
+      float2 acc[P];
+#pragma unroll
+      for (int p = 0; p < P; ++p) acc[p] = make_float2(0.f, 0.f);
+      const float2* row = s_mid + rp * G::RXQ + pad8(g);
+      // g is a multiple of 8, so pad8(g + q) = pad8(g) + pad8(q)
+      chain2(acc, wx, a.px.K, a.px.skip, [&](int q) { return row[pad8(q)]; });
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const long long yy = y0 + 2 * rp + h;
+        if (yy >= a.Y) continue;
+        D* orow = out + yy * a.X + x0 + g;
+        const long long left = a.X - (x0 + g);
+        float v[P];
+#pragma unroll
+        for (int p = 0; p < P; ++p) v[p] = h ? acc[p].y : acc[p].x;
+        if (left >= P && ((reinterpret_cast<uintptr_t>(orow) & (sizeof(D) * 4 - 1)) == 0)) {
+          store4<D>(orow, v[0], v[1], v[2], v[3]);
+          store4<D>(orow + 4, v[4], v[5], v[6], v[7]);
+        } else {
+#pragma unroll
+          for (int p = 0; p < P; ++p)
+            if (p < left) orow[p] = out_cast<D>(v[p]);
+        }
+      }
+    }
+  }
+}
+
+template <class T, class D, int KB>
+int launch_slab_kb(SlabArgs& a, cudaStream_t st) {
+  using G = Geom<T, KB>;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    cudaFuncSetAttribute(k_slab<T, D, KB, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         kMaxSmem);
+    cudaFuncSetAttribute(k_slab<T, D, KB, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         kMaxSmem);
+  });
+  a.tiles_x = (a.X + kSlabTX - 1) / kSlabTX;
+  a.tiles_y = (a.Y + kSlabTY - 1) / kSlabTY;
+  const long long blocks = a.B * a.tiles_x * a.tiles_y;
+  if (blocks == 0) return CIMX_OK;
+  a.status = device_status_word();
+  CUtensorMap map;
+  std::memset(&map, 0, sizeof(map));
+  const bool tma = make_tensor_map_3d(&map, a.in, dt_code<T>(), a.X, a.Y, a.B, G::BX, G::BY);
+  if (tma)
+    k_slab<T, D, KB, true><<<(unsigned)blocks, 256, G::SMEM, st>>>(map, a);
+  else
+    k_slab<T, D, KB, false><<<(unsigned)blocks, 256, G::SMEM, st>>>(map, a);
+  return cuda_fail(cudaGetLastError(), "slab launch");
+}
+
+template <class T, class D>
+int launch_slab_td(SlabArgs& a, cudaStream_t st) {
+  if (!a.has_y) return CIMX_FUSED_DECLINED;
+  const int k8 = std::max(a.py.K8, a.has_x ? a.px.K8 : 0);
+  if (k8 <= 8) return launch_slab_kb<T, D, 8>(a, st);
+  if (k8 <= 16) return launch_slab_kb<T, D, 16>(a, st);
+  if (k8 <= 24) return launch_slab_kb<T, D, 24>(a, st);
+  if (k8 <= 32) return launch_slab_kb<T, D, 32>(a, st);
+  if (k8 <= 40) return launch_slab_kb<T, D, 40>(a, st);
+  if (k8 <= 48) return launch_slab_kb<T, D, 48>(a, st);
+  return launch_slab_kb<T, D, 64>(a, st);
+}
+
+}  // namespace fast
+}  // namespace cimx

@@ -1,0 +1,25 @@
+// cimx_fast_u16.cu — instantiations of the fast kernels (cimx_fast.cuh) for
+// uint16_t input. Split by input dtype so the kernels compile in parallel.
+#include "cimx_fast.cuh"
+
+namespace cimx {
+
+int launch_stream_u16(const PassDesc& d, const float* w, int K, int anchor,
+                      bool interior_zero, const void* in, int tout, void* out,
+                      cudaStream_t st) {
+  using namespace fast;
+  if (tout == DT_F32)
+    return launch_stream_td<uint16_t, float>(d, w, K, anchor, interior_zero, in, out, st);
+  if (tout == DT_U16)
+    return launch_stream_td<uint16_t, uint16_t>(d, w, K, anchor, interior_zero, in, out, st);
+  return CIMX_FUSED_DECLINED;
+}
+
+int launch_slab_u16(SlabArgs& a, int tout, cudaStream_t st) {
+  using namespace fast;
+  if (tout == DT_F32) return launch_slab_td<uint16_t, float>(a, st);
+  if (tout == DT_U16) return launch_slab_td<uint16_t, uint16_t>(a, st);
+  return CIMX_FUSED_DECLINED;
+}
+
+}  // namespace cimx

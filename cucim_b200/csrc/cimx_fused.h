@@ -1,22 +1,58 @@
-// cimx_fused.h — entry into the fused multi-pass kernels (cimx_fused.cu).
+// cimx_fused.h — entry into the fast kernels of the plain path
+// (cimx_fast.cuh, instantiated per input dtype in cimx_fast_{f32,u16,u8}.cu)
+// and the dispatcher that decides whether a pass list can use them
+// (cimx_fused.cu).
 #pragma once
 
 #include "cimx_internal.h"
 
 namespace cimx {
 
-// Returned by try_fused when no fused kernel covers the pass list; the
-// caller then runs the passes one launch at a time.
+// Returned by try_fused when no fast kernel covers the pass list; the caller
+// then runs the passes one launch at a time.
 constexpr int CIMX_FUSED_DECLINED = 1;
 
+constexpr int kSlabMaxK = 64;  // longest pass the slab kernel takes
+
+// One pass of the slab kernel (float32 weights, already trimmed).
+struct SlabPass {
+  int K, K8, anchor, mode;
+  double cval;
+  int cval_as_input, dt, skip, pad;
+  float w[kSlabMaxK];
+};
+
+struct SlabArgs {
+  const void* in;
+  void* out;
+  long long B, Y, X;
+  long long tiles_x, tiles_y;
+  int has_y, has_x;
+  int* status;  // device status word for bounded waits
+  SlabPass py, px;
+};
+
 // Runs the whole pass list `ds` (already resolved against the input shape)
-// in fused launches when a fused kernel covers it. Returns CIMX_OK, a
-// negative error, or CIMX_FUSED_DECLINED.
+// in fast launches when they cover it. Returns CIMX_OK, a negative error, or
+// CIMX_FUSED_DECLINED (nothing was launched).
 int try_fused(const CimxArray* in, const CimxArray* out, PassDesc* ds, int npasses,
               cudaStream_t stream);
 
 // elementwise copy with conversion (used when a filter has no passes)
 int launch_copy_cast(const void* in, int tin, void* out, int tout, int64_t n,
                      cudaStream_t stream);
+
+// stream pass along a strided axis, by input dtype; K in {3,5,7,9,13,17}
+int launch_stream_f32(const PassDesc& d, const float* w, int K, int anchor, bool interior_zero,
+                      const void* in, int tout, void* out, cudaStream_t st);
+int launch_stream_u16(const PassDesc& d, const float* w, int K, int anchor, bool interior_zero,
+                      const void* in, int tout, void* out, cudaStream_t st);
+int launch_stream_u8(const PassDesc& d, const float* w, int K, int anchor, bool interior_zero,
+                     const void* in, int tout, void* out, cudaStream_t st);
+
+// fused (y, x) slab launch, by input dtype
+int launch_slab_f32(SlabArgs& a, int tout, cudaStream_t st);
+int launch_slab_u16(SlabArgs& a, int tout, cudaStream_t st);
+int launch_slab_u8(SlabArgs& a, int tout, cudaStream_t st);
 
 }  // namespace cimx

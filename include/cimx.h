@@ -101,6 +101,12 @@ CIMX_API int cimx_abi_version(void);
 /* Description of the last error raised on the calling thread. */
 CIMX_API const char* cimx_last_error_string(void);
 
+/* Status word of the current device: 0, or CIMX_E_TIMEOUT if a bounded
+ * device-side wait (TMA tile loads) gave up since the last clear. Reads the
+ * word synchronously; clear != 0 resets it. No counterpart in cuCIM, whose
+ * kernels have no device-side waits. */
+CIMX_API int cimx_device_status(int clear);
+
 /* Scratch allocator hook (default: cudaMallocAsync / cudaFreeAsync on the
  * call's stream). Both functions receive the stream the call runs on. */
 typedef void* (*cimx_alloc_fn)(size_t nbytes, void* stream, void* user);
