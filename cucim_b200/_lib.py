@@ -79,6 +79,9 @@ _sigs = {
     "cimx_separable": (
         [_A, _A, _P(CimxPass), ctypes.c_int, ctypes.c_int, ctypes.c_void_p], ctypes.c_int,
     ),
+    "cimx_separable_noalloc": (
+        [_A, _A, _P(CimxPass), ctypes.c_int, ctypes.c_void_p], ctypes.c_int,
+    ),
     "cimx_gradient_magnitude": (
         [_A, _A, _P(CimxPass), ctypes.c_int, ctypes.c_int, ctypes.c_void_p], ctypes.c_int,
     ),

@@ -133,6 +133,23 @@ CIMX_API int cimx_correlate1d(const CimxArray* in, const CimxArray* out, const d
 CIMX_API int cimx_separable(const CimxArray* in, const CimxArray* out, const CimxPass* passes,
                    int npasses, int lib_flags, void* stream);
 
+/* cimx_separable for callers that cannot allocate device memory (code
+ * running inside someone else's stream capture, plug-ins whose host
+ * application owns every allocation, pipelines that forbid allocation after
+ * start-up). No counterpart in cuCIM: it is an addition of this library.
+ * Same arguments and results as cimx_separable, but the passes run one
+ * launch each and the ping-pong intermediate lives in a 64 MiB static device
+ * array that every GPU loading the library holds until exit; the call makes
+ * no cudaMalloc/cudaFree or other allocating call. Limits: the intermediate
+ * (element count x output itemsize, needed when npasses >= 2) must fit in
+ * 64 MiB and each pass may have at most 1024 float32 / 512 float64 taps;
+ * larger requests return CIMX_E_INVALID with a message. The first call on a
+ * device resolves the array's device address (cudaGetSymbolAddress) and
+ * should come before any stream capture. All calls share the one array:
+ * calls that overlap on the GPU (concurrent streams) race on it. */
+CIMX_API int cimx_separable_noalloc(const CimxArray* in, const CimxArray* out,
+                                    const CimxPass* passes, int npasses, void* stream);
+
 /* out = sqrt(sum_i d_i^2) with d_i = separable(in, passes[i*passes_per_axis ...]),
  * i = 0..naxes-1, with cuCIM's rounding order: out = d_0*d_0 (rounded),
  * then out += (d_i*d_i rounded) for i >= 1, then sqrt. Replaces
