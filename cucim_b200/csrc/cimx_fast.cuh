@@ -131,14 +131,12 @@ __global__ void __launch_bounds__(256) k_stream(const StreamArgs<K> a) {
   extern __shared__ __align__(16) unsigned char sm_stream[];
   // this thread's prefetch slots: slot d at pre + d * 256 * 4
   T* pre = reinterpret_cast<T*>(sm_stream) + threadIdx.x * 4;
-  const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long long i4n = a.inner >> 2;
-  const long long i4 = tid % i4n;
-  const long long rest = tid / i4n;
-  const long long c = rest % a.nchunks;
-  const long long o = rest / a.nchunks;
-  if (o >= a.outer) return;  // no barrier in this kernel
-  const long long l0 = c * a.chunk;
+  // grid = (inner/4 in blocks of 256, chunks of L, outer); outer beyond the
+  // grid's z extent is visited by striding
+  const long long i4 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i4 >= (a.inner >> 2)) return;  // no barrier in this kernel
+  const long long l0 = (long long)blockIdx.y * a.chunk;
+  for (long long o = blockIdx.z; o < a.outer; o += gridDim.z) {
   const long long l1 = min(l0 + a.chunk, a.L);
   const T* in = static_cast<const T*>(a.in) + (o * a.L) * a.inner + i4 * 4;
   D* out = static_cast<D*>(a.out) + (o * a.L) * a.inner + i4 * 4;
@@ -206,6 +204,7 @@ __global__ void __launch_bounds__(256) k_stream(const StreamArgs<K> a) {
     }
   }
   cp_wait<0>();
+  }
 }
 
 template <class T, class D, int K>
@@ -239,13 +238,14 @@ int launch_stream_k(const PassDesc& d, const float* w, int anchor, bool interior
   while (chunk > 8 && lanes * ((d.L + chunk - 1) / chunk) < 148LL * 2048 * 2) chunk /= 2;
   a.chunk = chunk;
   a.nchunks = (d.L + chunk - 1) / chunk;
-  const long long threads = lanes * a.nchunks;
-  const unsigned blocks = (unsigned)((threads + 255) / 256);
+  if (a.nchunks > 65535) return CIMX_FUSED_DECLINED;
+  const dim3 grid((unsigned)((d.inner / 4 + 255) / 256), (unsigned)a.nchunks,
+                  (unsigned)std::min<long long>(d.outer, 65535));
   constexpr int smem = stream_smem<T, K>();
   if (interior_zero)
-    k_stream<T, D, K, true><<<blocks, 256, smem, st>>>(a);
+    k_stream<T, D, K, true><<<grid, 256, smem, st>>>(a);
   else
-    k_stream<T, D, K, false><<<blocks, 256, smem, st>>>(a);
+    k_stream<T, D, K, false><<<grid, 256, smem, st>>>(a);
   return cuda_fail(cudaGetLastError(), "stream pass launch");
 }
 
@@ -271,72 +271,139 @@ constexpr int kSlabTX = 128;   // output columns per tile
 __host__ __device__ constexpr int pad8(int c) { return c + (c >> 3); }
 
 // Compile-time tile geometry for taps bucket KB (both passes have K8 <= KB).
-// Shared memory: mbarrier | y taps | x taps (float2 pairs (t, t)) |
-// s_in (float, dense, RY x RX) | union { TMA tile (T, BY x BX),
-// s_mid (float2 row pairs, TY/2 x RXQ, columns at pad8(c)) }.
+//
+// Staged region: RY rows x RX columns starting at (y0 - ay, x0 - ax). Column
+// pairs (2m, 2m+1) of the y pass are aligned in the buffer the y pass reads:
+// the TMA tile (float input; its start column is 16-byte aligned, so the
+// staged region starts at an offset `off` and pairs are taken from
+// off - sh, sh = off & 1) or the converted tile s_in (other inputs, sh = 0).
+// Shared memory:
+//   mbarrier | y taps, x taps as (t, t) pairs |
+//   float input: raw x 2 (BY x BX floats each; the next slab's tile loads
+//                while this one is computed) | s_mid (TY/2 row pairs x RXQ float2)
+//   other input: s_in (RY x RXS floats) | union { raw (T), s_mid }
 template <class T, int KB>
 struct Geom {
+  static constexpr bool F32 = sizeof(T) == 4;
   static constexpr int RY = kSlabTY + KB;         // staged rows
   static constexpr int RX = kSlabTX + KB;         // staged columns (even)
-  static constexpr int RXQ = pad8(RX) + 1;        // float2 row-pair stride of s_mid
+  static constexpr int NPAIR = RX / 2 + 1;        // y-pass column pairs (one spare for sh)
+  static constexpr int RXS = RX + 2;              // s_in row stride (floats)
+  static constexpr int RXQ = pad8(RX + 2);        // s_mid row-pair stride (float2)
   static constexpr int VE = 16 / (int)sizeof(T);  // elements per 16 bytes
-  static constexpr int BX = (RX + VE - 1 + VE - 1) / VE * VE;  // TMA box width
+  static constexpr int BX = (RX + VE + VE - 1) / VE * VE;  // TMA box width >= RX + off + 1
   static constexpr int BY = RY;                   // TMA box height
   static constexpr int RAW = BX * BY * (int)sizeof(T);
   static constexpr int MID = (kSlabTY / 2) * RXQ * 8;
   static constexpr int OFF_W = 128;
-  static constexpr int OFF_IN = OFF_W + 2 * kSlabMaxK * 8;
-  static constexpr int SZ_IN = RY * RX * 4;
-  static constexpr int OFF_U = (OFF_IN + SZ_IN + 127) / 128 * 128;
-  static constexpr int SZ_U = RAW > MID ? RAW : MID;
-  static constexpr int SMEM = OFF_U + SZ_U;
-  static_assert(SZ_IN >= MID, "s_mid must fit in s_in's space");
+  static constexpr int RAWP = (RAW + 127) / 128 * 128;
+  // one TMA buffer: measured faster than two (two cost a resident CTA per SM)
+  static constexpr int NBUF = 1;
+  static constexpr int OFF_A = OFF_W + 2 * KB * 8;  // raw (f32) or s_in
+  static constexpr int SZ_A = F32 ? NBUF * RAWP : RY * RXS * 4;
+  static constexpr int OFF_B = (OFF_A + SZ_A + 127) / 128 * 128;  // s_mid (f32) or union
+  static constexpr int SZ_B = F32 ? MID : (RAW > MID ? RAW : MID);
+  static constexpr int SMEM = OFF_B + SZ_B;
 };
 
 __device__ __forceinline__ long long floor_div(long long a, long long b) {
   return a >= 0 ? a / b : -((-a + b - 1) / b);
 }
 
-// One fused multiply-add chain per lane pair for P outputs: acc[p] +=
-// x[p + k] * w[k], k ascending. `at(q)` returns the staged input pair at
-// window offset q. Full chunks of P taps run without guards, two chunks per
-// iteration so that the window halves swap roles without register moves.
+// Two float32 lanes in one 64-bit register (x in the low half).
+using f2 = unsigned long long;
+
+__device__ __forceinline__ f2 pack2(float x, float y) {
+  return (static_cast<f2>(__float_as_uint(y)) << 32) | __float_as_uint(x);
+}
+__device__ __forceinline__ float lo2(f2 v) { return __uint_as_float(static_cast<unsigned>(v)); }
+__device__ __forceinline__ float hi2(f2 v) {
+  return __uint_as_float(static_cast<unsigned>(v >> 32));
+}
+
+// d = fma(a, b, c) on both lanes, each an IEEE float32 FMA rounded to nearest
+// (bit-identical to fmaf on each lane).
+__device__ __forceinline__ f2 fma2(f2 a, f2 b, f2 c) {
+  f2 d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+
+// One fused multiply-add chain per lane for P outputs: acc[p] += x[p+k] w[k],
+// k ascending. `at(qb, j)` returns the staged input pair at window offset
+// qb + j, where qb is a multiple of P and j < P is a compile-time constant
+// (so the accessor computes its address once per chunk); w2 holds (t, t)
+// pairs. Full chunks of P taps run without guards, two chunks per iteration
+// so the window halves swap roles without register moves.
 template <class At>
-__device__ __forceinline__ void chain2(float2 (&acc)[P], const float2* w2, int K, int skip,
-                                       At at) {
-  float2 win[2 * P];
+__device__ __forceinline__ void chain2(f2 (&acc)[P], const f2* w2, int K, int skip, At at) {
+  f2 win[2 * P];
 #pragma unroll
-  for (int j = 0; j < P; ++j) win[j] = at(j);
+  for (int j = 0; j < P; ++j) win[j] = at(0, j);
   int k0 = 0;
   if (!skip) {
     for (; k0 + 2 * P <= K; k0 += 2 * P) {
 #pragma unroll
-      for (int j = 0; j < P; ++j) win[P + j] = at(k0 + P + j);
+      for (int j = 0; j < P; ++j) win[P + j] = at(k0 + P, j);
 #pragma unroll
       for (int j = 0; j < P; ++j) {
-        const float2 t = w2[k0 + j];
+        const f2 t = w2[k0 + j];
 #pragma unroll
-        for (int p = 0; p < P; ++p) acc[p] = ffma2(win[p + j], t, acc[p]);
+        for (int p = 0; p < P; ++p) acc[p] = fma2(win[p + j], t, acc[p]);
       }
 #pragma unroll
-      for (int j = 0; j < P; ++j) win[j] = at(k0 + 2 * P + j);
+      for (int j = 0; j < P; ++j) win[j] = at(k0 + 2 * P, j);
 #pragma unroll
       for (int j = 0; j < P; ++j) {
-        const float2 t = w2[k0 + P + j];
+        const f2 t = w2[k0 + P + j];
 #pragma unroll
-        for (int p = 0; p < P; ++p) acc[p] = ffma2(win[(P + p + j) % (2 * P)], t, acc[p]);
+        for (int p = 0; p < P; ++p) acc[p] = fma2(win[(P + p + j) % (2 * P)], t, acc[p]);
       }
     }
+    if (k0 + P <= K) {
+#pragma unroll
+      for (int j = 0; j < P; ++j) win[P + j] = at(k0 + P, j);
+#pragma unroll
+      for (int j = 0; j < P; ++j) {
+        const f2 t = w2[k0 + j];
+#pragma unroll
+        for (int p = 0; p < P; ++p) acc[p] = fma2(win[p + j], t, acc[p]);
+      }
+#pragma unroll
+      for (int j = 0; j < P; ++j) win[j] = win[P + j];
+      k0 += P;
+    }
   }
+  if (!skip && k0 < K) {
+    // last partial chunk: r = K - k0 taps, unrolled per r without guards
+#pragma unroll
+    for (int j = 0; j < P; ++j) win[P + j] = at(k0 + P, j);
+    const int r = K - k0;
+#define CIMX_TAIL(R)                                                         \
+  case R:                                                                    \
+    _Pragma("unroll") for (int j = 0; j < R; ++j) {                          \
+      const f2 t = w2[k0 + j];                                               \
+      _Pragma("unroll") for (int p = 0; p < P; ++p) acc[p] = fma2(win[p + j], t, acc[p]); \
+    }                                                                        \
+    break;
+    switch (r) {
+      CIMX_TAIL(1) CIMX_TAIL(2) CIMX_TAIL(3) CIMX_TAIL(4) CIMX_TAIL(5) CIMX_TAIL(6)
+      CIMX_TAIL(7)
+      default: break;
+    }
+#undef CIMX_TAIL
+    return;
+  }
+  // every chunk with guards when zero taps must be skipped
   for (; k0 < K; k0 += P) {
 #pragma unroll
-    for (int j = 0; j < P; ++j) win[P + j] = at(k0 + P + j);
+    for (int j = 0; j < P; ++j) win[P + j] = at(k0 + P, j);
 #pragma unroll
     for (int j = 0; j < P; ++j) {
-      const float2 t = w2[k0 + j];
-      if (k0 + j < K && (!skip || t.x != 0.f)) {
+      const f2 t = w2[k0 + j];
+      if (k0 + j < K && (!skip || lo2(t) != 0.f)) {
 #pragma unroll
-        for (int p = 0; p < P; ++p) acc[p] = ffma2(win[p + j], t, acc[p]);
+        for (int p = 0; p < P; ++p) acc[p] = fma2(win[p + j], t, acc[p]);
       }
     }
 #pragma unroll
@@ -347,8 +414,7 @@ __device__ __forceinline__ void chain2(float2 (&acc)[P], const float2* w2, int K
 // Value of the staged element (gy, gx) of the slab, boundary modes applied.
 template <class T>
 __device__ __forceinline__ float staged_value(const T* in, long long gy, long long gx,
-                                              const SlabArgs& a, int my, int mx, float cy,
-                                              float cx) {
+                                              const SlabArgs& a, int my, int mx, float cy) {
   long long yy = gy, xx = gx;
   if (gy < 0 || gy >= a.Y) yy = map_coord(gy, a.Y, my);
   if (gx < 0 || gx >= a.X) xx = map_coord(gx, a.X, mx);
@@ -362,127 +428,159 @@ __global__ void __launch_bounds__(256) k_slab(const __grid_constant__ CUtensorMa
                                                const SlabArgs a) {
   using G = Geom<T, KB>;
   extern __shared__ __align__(128) unsigned char smem[];
-  uint64_t* bar = reinterpret_cast<uint64_t*>(smem);
-  float2* wy = reinterpret_cast<float2*>(smem + G::OFF_W);
-  float2* wx = wy + kSlabMaxK;
-  float* s_in = reinterpret_cast<float*>(smem + G::OFF_IN);
-  T* raw = reinterpret_cast<T*>(smem + G::OFF_U);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem);  // bar[0], bar[1]: one per raw buffer
+  f2* wy = reinterpret_cast<f2*>(smem + G::OFF_W);
+  f2* wx = wy + KB;
+  T* raw0 = reinterpret_cast<T*>(smem + (G::F32 ? G::OFF_A : G::OFF_B));
+  float* s_in = reinterpret_cast<float*>(smem + G::OFF_A);  // non-float inputs only
+  f2* s_mid = reinterpret_cast<f2*>(smem + G::OFF_B);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 
-  long long bid = blockIdx.x;
-  const long long tx = bid % a.tiles_x;
-  bid /= a.tiles_x;
-  const long long ty = bid % a.tiles_y;
-  const long long b = bid / a.tiles_y;
-  const long long y0 = ty * kSlabTY, x0 = tx * kSlabTX;
+  if (TMA && threadIdx.x == 0) {
+    mbar_init(bar, 1);
+    mbar_init(bar + 1, 1);
+    mbar_fence_init();
+  }
+  for (int k = threadIdx.x; k < KB; k += blockDim.x) {
+    const float ty_ = k < a.py.K ? a.py.w[k] : 0.f;
+    const float tx_ = (a.has_x && k < a.px.K) ? a.px.w[k] : 0.f;
+    wy[k] = pack2(ty_, ty_);
+    wx[k] = pack2(tx_, tx_);
+  }
+  __syncthreads();
+
   const int ay = a.py.anchor;
   const int ax = a.has_x ? a.px.anchor : 0;
-  const long long ys = y0 - ay, xst = x0 - ax;
-  const T* in = static_cast<const T*>(a.in) + b * a.Y * a.X;
-  D* out = static_cast<D*>(a.out) + b * a.Y * a.X;
   const int my = a.py.mode;
   const int mx = a.has_x ? a.px.mode : CIMX_MODE_NEAREST;
   const float cy = fill_value<float>(a.py.cval, a.py.cval_as_input, a.py.dt);
   const float cx = a.has_x ? fill_value<float>(a.px.cval, a.px.cval_as_input, a.px.dt) : 0.f;
-
-  // a tile whose staged region lies inside the array needs no boundary work
-  const bool interior = ys >= 0 && ys + G::RY <= a.Y && xst >= 0 && xst + G::RX <= a.X;
+  // grid = (tiles_x, tiles_y, slabs); slabs beyond the grid's z extent are
+  // visited by striding, the mbarrier phase flipping once per slab
+  const long long y0 = (long long)blockIdx.y * kSlabTY, x0 = (long long)blockIdx.x * kSlabTX;
+  const long long ys = y0 - ay, xst = x0 - ax;
   const long long xs = floor_div(xst, G::VE) * G::VE;  // 16-byte aligned TMA start column
   const int off = static_cast<int>(xst - xs);
-
-  if (TMA && threadIdx.x == 0) {
-    mbar_init(bar, 1);
-    mbar_fence_init();
-  }
-  for (int k = threadIdx.x; k < kSlabMaxK; k += blockDim.x) {
-    const float ty_ = k < a.py.K ? a.py.w[k] : 0.f;
-    const float tx_ = (a.has_x && k < a.px.K) ? a.px.w[k] : 0.f;
-    wy[k] = make_float2(ty_, ty_);
-    wx[k] = make_float2(tx_, tx_);
-  }
-  __syncthreads();
+  // float input: pairs are read from the TMA tile starting at column off - sh
+  const int sh = (TMA && G::F32) ? (off & 1) : 0;
+  // staged columns [cl, cr) and rows [rl, rr) lie inside the array
+  auto clampi = [](long long v, long long lo, long long hi) {
+    return static_cast<int>(v < lo ? lo : (v > hi ? hi : v));
+  };
+  const int cl = clampi(-xst, 0, G::RX);
+  const int cr = clampi(a.X - xst, cl, G::RX);
+  const int rl = clampi(-ys, 0, G::RY);
+  const int rr = clampi(a.Y - ys, rl, G::RY);
+  // float input: two TMA buffers; the copy for the next slab is issued before
+  // the current slab is computed. Other inputs: one buffer.
+  constexpr int NBUF = G::NBUF;
+  auto issue = [&](long long bb, int k) {
+    fence_proxy_async_smem();  // earlier reads of this buffer came first
+    mbar_expect_tx(bar + k, G::RAW);
+    tma_load_3d(reinterpret_cast<unsigned char*>(raw0) + k * G::RAWP, &map, bar + k,
+                static_cast<int>(xs), static_cast<int>(ys), static_cast<int>(bb));
+  };
+  if (TMA && NBUF == 2 && threadIdx.x == 0 && blockIdx.z < a.B) issue(blockIdx.z, 0);
+  long long it = 0;
+  for (long long b = blockIdx.z; b < a.B; b += gridDim.z, ++it) {
+  const T* in = static_cast<const T*>(a.in) + b * a.Y * a.X;
+  D* out = static_cast<D*>(a.out) + b * a.Y * a.X;
+  const int kb = static_cast<int>(it % NBUF);
+  T* raw = reinterpret_cast<T*>(reinterpret_cast<unsigned char*>(raw0) + kb * G::RAWP);
 
   // 1. stage the tile
-  bool from_raw = false;  // the y pass reads the TMA tile directly
   if (TMA) {
+    // thread 0 prefetches the next slab's tile (double buffering, float input)
+    // and waits (bounded) for this one; the others wait at the barrier, where
+    // they issue no instructions
+    int ok = 1;
     if (threadIdx.x == 0) {
-      mbar_expect_tx(bar, G::RAW);
-      tma_load_3d(raw, &map, bar, static_cast<int>(xs), static_cast<int>(ys),
-                  static_cast<int>(b));
+      if (NBUF == 2 && b + gridDim.z < a.B) issue(b + gridDim.z, 1 - kb);
+      if (NBUF == 1) issue(b, 0);
+      const uint32_t parity = static_cast<uint32_t>((it / NBUF) & 1);
+      ok = mbar_wait(bar + kb, parity, a.status) ? 1 : 0;
     }
-    if (!mbar_wait(bar, 0, a.status)) return;
-    from_raw = interior;
-    if (!from_raw) {
-      // convert to float and apply the boundary modes
+    if (!__syncthreads_and(ok)) return;
+  }
+  if (G::F32 && TMA) {
+    // the tile is already float: rewrite only the staged elements that lie
+    // outside the array with their boundary-mode values
+    if (!(rl == 0 && rr == G::RY && cl == 0 && cr == G::RX)) {
+      float* rawf = reinterpret_cast<float*>(raw);
       for (int r = warp; r < G::RY; r += 8) {
-        const long long gy = ys + r;
-        const bool yin = gy >= 0 && gy < a.Y;
-        for (int c = lane; c < G::RX; c += 32) {
-          const long long gx = xst + c;
-          float v;
-          if (yin && gx >= 0 && gx < a.X) v = static_cast<float>(raw[r * G::BX + off + c]);
-          else v = staged_value<T>(in, gy, gx, a, my, mx, cy, cx);
-          s_in[r * G::RX + c] = v;
+        float* row = rawf + r * G::BX + off;
+        if (r < rl || r >= rr) {
+          for (int c = lane; c < G::RX; c += 32)
+            row[c] = staged_value<T>(in, ys + r, xst + c, a, my, mx, cy);
+        } else {
+          for (int c = lane; c < cl; c += 32)
+            row[c] = staged_value<T>(in, ys + r, xst + c, a, my, mx, cy);
+          for (int c = cr + lane; c < G::RX; c += 32)
+            row[c] = staged_value<T>(in, ys + r, xst + c, a, my, mx, cy);
         }
       }
     }
   } else {
+    // convert to float into the staging buffer at column c (pairs aligned)
+    float* dst = G::F32 ? reinterpret_cast<float*>(raw) : s_in;
+    const int stride = G::F32 ? G::BX : G::RXS;
     for (int r = warp; r < G::RY; r += 8) {
-      const long long gy = ys + r;
-      for (int c = lane; c < G::RX; c += 32)
-        s_in[r * G::RX + c] = staged_value<T>(in, gy, xst + c, a, my, mx, cy, cx);
+      const bool row_in = r >= rl && r < rr;
+      for (int c = lane; c < G::RX; c += 32) {
+        float v;
+        if (TMA && row_in && c >= cl && c < cr) v = static_cast<float>(raw[r * G::BX + off + c]);
+        else v = staged_value<T>(in, ys + r, xst + c, a, my, mx, cy);
+        dst[r * stride + c] = v;
+      }
     }
   }
   __syncthreads();
 
-  // the y result goes where nothing is read any more: s_in's space when the
-  // y pass reads the TMA tile, the TMA tile's space otherwise
-  float2* s_mid = reinterpret_cast<float2*>(from_raw ? smem + G::OFF_IN : smem + G::OFF_U);
-
-  // 2. y pass: one column pair x P rows per item
+  // 2. y pass: one column pair x P rows per item, written to s_mid as row
+  //    pairs (rounded through D); column index e = staged column + sh
   {
-    constexpr int pairs = G::RX / 2;
+    const float* src = G::F32 ? reinterpret_cast<const float*>(raw) : s_in;
+    const int stride = G::F32 ? G::BX : G::RXS;
+    const int soff = (G::F32 && TMA) ? off - sh : 0;
+    const int npair = (G::RX + sh + 1) / 2;
     constexpr int groups = kSlabTY / P;
-    for (int item = threadIdx.x; item < pairs * groups; item += blockDim.x) {
-      const int c = 2 * (item % pairs);
-      const int rg = (item / pairs) * P;
-      float2 acc[P];
+    for (int item = threadIdx.x; item < G::NPAIR * groups; item += blockDim.x) {
+      const int m = item % G::NPAIR;
+      const int rg = (item / G::NPAIR) * P;
+      if (m >= npair) continue;
+      const int e = 2 * m;
+      f2 acc[P];
 #pragma unroll
-      for (int p = 0; p < P; ++p) acc[p] = make_float2(0.f, 0.f);
-      if (from_raw) {
-        const T* col = raw + rg * G::BX + off + c;
-        chain2(acc, wy, a.py.K, a.py.skip, [&](int q) {
-          return make_float2(static_cast<float>(col[q * G::BX]),
-                             static_cast<float>(col[q * G::BX + 1]));
-        });
-      } else {
-        const float2* col = reinterpret_cast<const float2*>(s_in + rg * G::RX + c);
-        chain2(acc, wy, a.py.K, a.py.skip, [&](int q) { return col[q * (G::RX / 2)]; });
-      }
+      for (int p = 0; p < P; ++p) acc[p] = 0ull;
+      const f2* col = reinterpret_cast<const f2*>(src + rg * stride + soff + e);
+      chain2(acc, wy, a.py.K, a.py.skip,
+             [&](int qb, int j) { return col[(qb + j) * (stride / 2)]; });
+      const long long gx = xst + e - sh;
       if (a.has_x) {
-        const long long gx = xst + c;
         const bool f0 = mx == CIMX_MODE_CONSTANT && (gx < 0 || gx >= a.X);
         const bool f1 = mx == CIMX_MODE_CONSTANT && (gx + 1 < 0 || gx + 1 >= a.X);
-        float2* d0 = s_mid + (rg / 2) * G::RXQ + pad8(c);
-        float2* d1 = s_mid + (rg / 2) * G::RXQ + pad8(c + 1);
+        f2* d0 = s_mid + (rg / 2) * G::RXQ + pad8(e);
+        f2* d1 = s_mid + (rg / 2) * G::RXQ + pad8(e + 1);
 #pragma unroll
         for (int p = 0; p < P; p += 2) {
-          const float a0 = f0 ? cx : static_cast<float>(out_cast<D>(acc[p].x));
-          const float b0 = f0 ? cx : static_cast<float>(out_cast<D>(acc[p + 1].x));
-          const float a1 = f1 ? cx : static_cast<float>(out_cast<D>(acc[p].y));
-          const float b1 = f1 ? cx : static_cast<float>(out_cast<D>(acc[p + 1].y));
-          d0[(p / 2) * G::RXQ] = make_float2(a0, b0);
-          d1[(p / 2) * G::RXQ] = make_float2(a1, b1);
+          const float a0 = f0 ? cx : static_cast<float>(out_cast<D>(lo2(acc[p])));
+          const float b0 = f0 ? cx : static_cast<float>(out_cast<D>(lo2(acc[p + 1])));
+          const float a1 = f1 ? cx : static_cast<float>(out_cast<D>(hi2(acc[p])));
+          const float b1 = f1 ? cx : static_cast<float>(out_cast<D>(hi2(acc[p + 1])));
+          d0[(p / 2) * G::RXQ] = pack2(a0, b0);
+          d1[(p / 2) * G::RXQ] = pack2(a1, b1);
         }
-      } else if (c < kSlabTX) {
+      } else {
         // y only: store straight to the output
+        const long long c0 = e - sh;
 #pragma unroll
         for (int p = 0; p < P; ++p) {
           const long long yy = y0 + rg + p;
-          if (yy < a.Y) {
-            if (x0 + c < a.X) out[yy * a.X + x0 + c] = out_cast<D>(acc[p].x);
-            if (x0 + c + 1 < a.X) out[yy * a.X + x0 + c + 1] = out_cast<D>(acc[p].y);
-          }
+          if (yy >= a.Y) continue;
+          if (c0 >= 0 && c0 < kSlabTX && x0 + c0 < a.X)
+            out[yy * a.X + x0 + c0] = out_cast<D>(lo2(acc[p]));
+          if (c0 + 1 >= 0 && c0 + 1 < kSlabTX && x0 + c0 + 1 < a.X)
+            out[yy * a.X + x0 + c0 + 1] = out_cast<D>(hi2(acc[p]));
         }
       }
     }
@@ -490,17 +588,22 @@ __global__ void __launch_bounds__(256) k_slab(const __grid_constant__ CUtensorMa
 
   if (a.has_x) {
     __syncthreads();
-    // 3. x pass: one row pair x P consecutive outputs per item
+    // 3. x pass: one row pair x P consecutive outputs per item; output column
+    //    g + q reads s_mid column g + q + sh, and since g is a multiple of 8,
+    //    pad8(g + q + sh) = pad8(g) + pad8(q + sh)
     constexpr int gpr = kSlabTX / P;
     for (int item = threadIdx.x; item < (kSlabTY / 2) * gpr; item += blockDim.x) {
       const int rp = item / gpr;
       const int g = (item % gpr) * P;
-      float2 acc[P];
+      f2 acc[P];
 #pragma unroll
-      for (int p = 0; p < P; ++p) acc[p] = make_float2(0.f, 0.f);
-      const float2* row = s_mid + rp * G::RXQ + pad8(g);
-      // g is a multiple of 8, so pad8(g + q) = pad8(g) + pad8(q)
-      chain2(acc, wx, a.px.K, a.px.skip, [&](int q) { return row[pad8(q)]; });
+      for (int p = 0; p < P; ++p) acc[p] = 0ull;
+      const f2* row = s_mid + rp * G::RXQ + pad8(g);
+      if (sh)
+        chain2(acc, wx, a.px.K, a.px.skip,
+               [&](int qb, int j) { return row[pad8(qb) + (j + 1) + ((j + 1) >> 3)]; });
+      else
+        chain2(acc, wx, a.px.K, a.px.skip, [&](int qb, int j) { return row[pad8(qb) + j]; });
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
         const long long yy = y0 + 2 * rp + h;
@@ -509,7 +612,7 @@ __global__ void __launch_bounds__(256) k_slab(const __grid_constant__ CUtensorMa
         const long long left = a.X - (x0 + g);
         float v[P];
 #pragma unroll
-        for (int p = 0; p < P; ++p) v[p] = h ? acc[p].y : acc[p].x;
+        for (int p = 0; p < P; ++p) v[p] = h ? hi2(acc[p]) : lo2(acc[p]);
         if (left >= P && ((reinterpret_cast<uintptr_t>(orow) & (sizeof(D) * 4 - 1)) == 0)) {
           store4<D>(orow, v[0], v[1], v[2], v[3]);
           store4<D>(orow + 4, v[4], v[5], v[6], v[7]);
@@ -520,6 +623,8 @@ __global__ void __launch_bounds__(256) k_slab(const __grid_constant__ CUtensorMa
         }
       }
     }
+  }
+  __syncthreads();  // shared buffers are reused by the next slab
   }
 }
 
@@ -541,10 +646,20 @@ int launch_slab_kb(SlabArgs& a, cudaStream_t st) {
   CUtensorMap map;
   std::memset(&map, 0, sizeof(map));
   const bool tma = make_tensor_map_3d(&map, a.in, dt_code<T>(), a.X, a.Y, a.B, G::BX, G::BY);
+  // without TMA a float tile is staged by plain loads into the raw buffer
+  if (a.tiles_y > 65535) return CIMX_FUSED_DECLINED;
+  // enough CTAs to fill the GPU a few times; each walks a stride of slabs so
+  // that it can prefetch the next slab's tile while computing the current one
+  const long long per_slab = a.tiles_x * a.tiles_y;
+  const long long zs =
+      G::NBUF == 2 ? std::max<long long>(1, std::min<long long>(
+                                                {a.B, 65535LL, (148LL * 8 + per_slab - 1) / per_slab}))
+                   : std::min<long long>(a.B, 65535LL);
+  const dim3 grid((unsigned)a.tiles_x, (unsigned)a.tiles_y, (unsigned)zs);
   if (tma)
-    k_slab<T, D, KB, true><<<(unsigned)blocks, 256, G::SMEM, st>>>(map, a);
+    k_slab<T, D, KB, true><<<grid, 256, G::SMEM, st>>>(map, a);
   else
-    k_slab<T, D, KB, false><<<(unsigned)blocks, 256, G::SMEM, st>>>(map, a);
+    k_slab<T, D, KB, false><<<grid, 256, G::SMEM, st>>>(map, a);
   return cuda_fail(cudaGetLastError(), "slab launch");
 }
 
