@@ -84,10 +84,15 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}",
-                 "--format=csv,noheader,nounits", "-lms", "100"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            # nvidia-smi takes a moment to start; wait for its first sample
+            t0 = time.time()
+            while not self.rows and time.time() - t0 < 5.0 and self.proc.poll() is None:
+                time.sleep(0.02)
+            self.rows.clear()
         except OSError:
             self.proc = None
         return self
@@ -131,6 +136,21 @@ def step_ops(ndi, x, outs):
 LAUNCHES_PER_STEP = 10  # each op: one streamed pass (axis 0) + one fused (y, x) slab launch
 
 
+def reduce_step_time(ms, world, device, dist, torch):
+    """Max over ranks of the per-step device time (ms): the job is as slow as
+    its slowest replica."""
+    if world <= 1:
+        return ms
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_value(nvox, world, ms):
+    """Whole-job throughput in Gvox/s: every rank filters its own stack."""
+    return nvox * world / (ms * 1e-3) / 1e9
+
+
 def time_kernel(fn, reps, torch):
     """Average device time of fn() (one launch) with events on the current stream."""
     fn()
@@ -167,11 +187,11 @@ def run_ours(args, rank, world, local_rank):
     for _ in range(args.warmup):
         step_ops(ndi, x, outs)
     torch.cuda.synchronize()
-    barrier()
-    torch.cuda.synchronize()
     t0 = torch.cuda.Event(enable_timing=True)
     t1 = torch.cuda.Event(enable_timing=True)
     with ClockSampler(local_rank) as clk:
+        barrier()
+        torch.cuda.synchronize()
         t0.record()
         for _ in range(args.steps):
             step_ops(ndi, x, outs)
@@ -179,12 +199,8 @@ def run_ours(args, rank, world, local_rank):
         torch.cuda.synchronize()
     barrier()
     torch.cuda.synchronize()
-    ms = t0.elapsed_time(t1) / args.steps
-    if world > 1:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = nvox * world / (ms * 1e-3) / 1e9
+    ms = reduce_step_time(t0.elapsed_time(t1) / args.steps, world, dev, dist, torch)
+    value = aggregate_value(nvox, world, ms)
 
     # per-kernel timing: each call below is exactly one launch of the kernel
     # that runs inside the step (same shapes, same dtypes)
