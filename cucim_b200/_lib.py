@@ -15,7 +15,7 @@ LIB_PATH = os.path.join(_HERE, "_lib", "libcimx.so")
 if not os.path.exists(LIB_PATH):
     raise ImportError(
         f"libcimx.so not found at {LIB_PATH}; build it with "
-        "`python -m cucim_b200.build` (nvcc, sm_100a)"
+        "`python cucim_b200/build.py` (nvcc, sm_100a)"
     )
 
 lib = ctypes.CDLL(LIB_PATH)
