@@ -11,6 +11,7 @@
 #include "cimx_common.cuh"
 #include "cimx_internal.h"
 #include "cimx_fused.h"
+#include "cimx_tc.h"
 
 namespace cimx {
 
@@ -243,8 +244,9 @@ int cimx_separable(const CimxArray* in, const CimxArray* out, const CimxPass* pa
   }
   if (n == 0) return CIMX_OK;
 
+  const bool tensor = (lib_flags & CIMX_L_TENSOR_BF16X3) != 0;
   // fused kernels take whole runs of passes in one launch
-  if (!(lib_flags & CIMX_L_NO_FUSION)) {
+  if (!tensor && !(lib_flags & CIMX_L_NO_FUSION)) {
     rc = try_fused(in, out, ds.data(), npasses, st);
     if (rc != CIMX_FUSED_DECLINED) return rc;
     rc = CIMX_OK;
@@ -266,7 +268,10 @@ int cimx_separable(const CimxArray* in, const CimxArray* out, const CimxPass* pa
     ds[i].tin = tsrc;
     ds[i].out = dst;
     ds[i].tout = out->dtype;
-    rc = launch_generic_pass(ds[i], st);
+    if (tensor && ds[i].K >= 16 && tc_supports(ds[i]))
+      rc = launch_tc_pass(ds[i], st);
+    else
+      rc = launch_generic_pass(ds[i], st);
     src = dst;
     tsrc = out->dtype;
     dst = (dst == out->data) ? temp : out->data;

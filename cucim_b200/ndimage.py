@@ -83,6 +83,14 @@ def _build_passes(in_dtype, out_dtype, ndim, specs, cval, algorithm):
     return pl
 
 
+# algorithm="tensor": an addition of this library (cuCIM accepts only
+# "shared_memory", "elementwise" and None). float32 -> float32 passes with at
+# least 16 taps run on the tensor cores in BF16x3 split precision (banded
+# Toeplitz products, float32 accumulation); results are close to, not
+# bit-identical with, the float32 chain. Other passes run as usual.
+TENSOR = "tensor"
+
+
 def _run(input, specs, output, cval, algorithm=None):
     """Apply the pass list to `input` into `output` (FLT:363-396 semantics)."""
     x = _arrays.as_tensor(input)
@@ -91,12 +99,15 @@ def _run(input, specs, output, cval, algorithm=None):
     xc = x.contiguous()
     slot = _arrays.output_slot(output, input, xc)
     out_dt = slot.dtype
+    lib_flags = 0
+    if algorithm == TENSOR:
+        lib_flags, algorithm = _lib.L_TENSOR_BF16X3, None
     pl = _build_passes(_arrays.np_dtype(xc), out_dt, xc.dim(), specs, cval, algorithm)
     arr = pl.array()
     a_in = _arrays.to_cimx(xc)
     a_out = _arrays.to_cimx(slot.work)
-    rc = _lib.lib.cimx_separable(ctypes.byref(a_in), ctypes.byref(a_out), arr, len(pl), 0,
-                                 _arrays.stream_of(xc))
+    rc = _lib.lib.cimx_separable(ctypes.byref(a_in), ctypes.byref(a_out), arr, len(pl),
+                                 lib_flags, _arrays.stream_of(xc))
     _lib.check(rc, "separable filter")
     return slot.result()
 
@@ -108,7 +119,7 @@ def _correlate_or_convolve1d(input, weights, axis, output, mode, cval, origin,
     x = _arrays.as_tensor(input)
     axis = _util.normalize_axis(axis, x.dim())
     w = _weights_to_host(weights)
-    if algorithm not in (None, "shared_memory", "elementwise"):
+    if algorithm not in (None, "shared_memory", "elementwise", TENSOR):
         raise ValueError("algorithm must be 'shared_memory', 'elementwise' or None")
     if algorithm == "shared_memory" and mode == "constant" and (
         not np.isfinite(cval) or (cval < 0 and _arrays.np_dtype(x).kind == "u")

@@ -70,6 +70,10 @@ enum {
 /* Library-level flags for multi-pass calls. */
 enum {
   CIMX_L_NO_FUSION = 1 << 0,    /* force one launch per pass (ping-pong through scratch) */
+  CIMX_L_TENSOR_BF16X3 = 1 << 1,/* run float32 -> float32 passes with at least 16 taps on the
+                                   tensor cores: banded-Toeplitz products of bfloat16 hi/lo
+                                   splits, float32 accumulation (not bit-identical to the
+                                   float32 chain; an addition of this library) */
 };
 
 /* One 1-D correlation pass of a separable filter. */
