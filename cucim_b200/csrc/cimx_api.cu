@@ -244,7 +244,8 @@ int cimx_separable(const CimxArray* in, const CimxArray* out, const CimxPass* pa
   }
   if (n == 0) return CIMX_OK;
 
-  const bool tensor = (lib_flags & CIMX_L_TENSOR_BF16X3) != 0;
+  const bool tf32x3 = (lib_flags & CIMX_L_TENSOR_TF32X3) != 0;
+  const bool tensor = tf32x3 || (lib_flags & CIMX_L_TENSOR_BF16X3) != 0;
   // fused kernels take whole runs of passes in one launch
   if (!tensor && !(lib_flags & CIMX_L_NO_FUSION)) {
     rc = try_fused(in, out, ds.data(), npasses, st);
@@ -268,7 +269,9 @@ int cimx_separable(const CimxArray* in, const CimxArray* out, const CimxPass* pa
     ds[i].tin = tsrc;
     ds[i].out = dst;
     ds[i].tout = out->dtype;
-    if (tensor && ds[i].K >= 16 && tc_supports(ds[i]))
+    if (tf32x3 && ds[i].K >= 16 && tcs_supports(ds[i]))
+      rc = launch_tcs_pass(ds[i], st);
+    else if (tensor && !tf32x3 && ds[i].K >= 16 && tc_supports(ds[i]))
       rc = launch_tc_pass(ds[i], st);
     else
       rc = launch_generic_pass(ds[i], st);

@@ -32,7 +32,7 @@ int* g_status[64] = {nullptr};
 }  // namespace
 
 bool make_tensor_map_3d(CUtensorMap* map, const void* base, int dtype, long long X, long long Y,
-                        long long Z, int box_x, int box_y) {
+                        long long Z, int box_x, int box_y, bool swizzle128) {
   auto fn = encode_fn();
   if (!fn) return false;
   CUtensorMapDataType t;
@@ -45,6 +45,7 @@ bool make_tensor_map_3d(CUtensorMap* map, const void* base, int dtype, long long
   const long long es = dtype_size(dtype);
   if ((reinterpret_cast<uintptr_t>(base) & 15) != 0) return false;
   if ((X * es) % 16 != 0 || box_x * es % 16 != 0) return false;
+  if (swizzle128 && box_x * es > 128) return false;
   if (box_x > 256 || box_y > 256 || X >= (1ll << 32) || Y >= (1ll << 32) || Z >= (1ll << 32))
     return false;
   const cuuint64_t dims[3] = {(cuuint64_t)X, (cuuint64_t)Y, (cuuint64_t)Z};
@@ -53,7 +54,8 @@ bool make_tensor_map_3d(CUtensorMap* map, const void* base, int dtype, long long
   const cuuint32_t box[3] = {(cuuint32_t)box_x, (cuuint32_t)box_y, 1};
   const cuuint32_t estr[3] = {1, 1, 1};
   CUresult r = fn(map, t, 3, const_cast<void*>(base), dims, strides, box, estr,
-                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE,
+                  swizzle128 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_NONE,
                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS;
 }

@@ -74,8 +74,10 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, u
 
 // Host: encode a 3-D tiled tensor map over a C-contiguous (Z, Y, X) array.
 // Returns false when the layout is not TMA-eligible (alignment, extents).
+// swizzle128 selects the 128-byte shared-memory swizzle (box_x * element
+// size must then be at most 128 bytes and the destination 1024-byte aligned).
 bool make_tensor_map_3d(CUtensorMap* map, const void* base, int dtype, long long X, long long Y,
-                        long long Z, int box_x, int box_y);
+                        long long Z, int box_x, int box_y, bool swizzle128 = false);
 
 // Host: the current device's status word (device memory, allocated once).
 int* device_status_word();

@@ -83,12 +83,16 @@ def _build_passes(in_dtype, out_dtype, ndim, specs, cval, algorithm):
     return pl
 
 
-# algorithm="tensor": an addition of this library (cuCIM accepts only
-# "shared_memory", "elementwise" and None). float32 -> float32 passes with at
-# least 16 taps run on the tensor cores in BF16x3 split precision (banded
-# Toeplitz products, float32 accumulation); results are close to, not
+# algorithm="tensor" and "tensor_bf16x3": additions of this library (cuCIM
+# accepts only "shared_memory", "elementwise" and None). float32 -> float32
+# passes with at least 16 taps run on the tensor cores as banded-Toeplitz
+# products with float32 accumulation: "tensor" splits operands into tf32
+# hi + lo (TF32x3, max relative error near 1e-6), "tensor_bf16x3" into
+# bfloat16 hi + lo (BF16x3, near 1e-5). Results are close to, not
 # bit-identical with, the float32 chain. Other passes run as usual.
 TENSOR = "tensor"
+TENSOR_BF16X3 = "tensor_bf16x3"
+_TENSOR_FLAGS = {TENSOR: _lib.L_TENSOR_TF32X3, TENSOR_BF16X3: _lib.L_TENSOR_BF16X3}
 
 
 def _run(input, specs, output, cval, algorithm=None):
@@ -100,8 +104,8 @@ def _run(input, specs, output, cval, algorithm=None):
     slot = _arrays.output_slot(output, input, xc)
     out_dt = slot.dtype
     lib_flags = 0
-    if algorithm == TENSOR:
-        lib_flags, algorithm = _lib.L_TENSOR_BF16X3, None
+    if algorithm in _TENSOR_FLAGS:
+        lib_flags, algorithm = _TENSOR_FLAGS[algorithm], None
     pl = _build_passes(_arrays.np_dtype(xc), out_dt, xc.dim(), specs, cval, algorithm)
     arr = pl.array()
     a_in = _arrays.to_cimx(xc)
@@ -119,7 +123,7 @@ def _correlate_or_convolve1d(input, weights, axis, output, mode, cval, origin,
     x = _arrays.as_tensor(input)
     axis = _util.normalize_axis(axis, x.dim())
     w = _weights_to_host(weights)
-    if algorithm not in (None, "shared_memory", "elementwise", TENSOR):
+    if algorithm not in (None, "shared_memory", "elementwise", TENSOR, TENSOR_BF16X3):
         raise ValueError("algorithm must be 'shared_memory', 'elementwise' or None")
     if algorithm == "shared_memory" and mode == "constant" and (
         not np.isfinite(cval) or (cval < 0 and _arrays.np_dtype(x).kind == "u")

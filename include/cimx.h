@@ -74,6 +74,10 @@ enum {
                                    tensor cores: banded-Toeplitz products of bfloat16 hi/lo
                                    splits, float32 accumulation (not bit-identical to the
                                    float32 chain; an addition of this library) */
+  CIMX_L_TENSOR_TF32X3 = 1 << 2,/* the same on tf32 hi/lo splits (hi*hi + hi*lo + lo*hi), in a
+                                   streaming TMA-fed kernel: about ten times more accurate
+                                   than BF16X3 (a relative error per product near 2^-21) and
+                                   faster; takes precedence when both bits are set */
 };
 
 /* One 1-D correlation pass of a separable filter. */

@@ -1,7 +1,15 @@
-"""The split-precision tensor-core path (algorithm="tensor"): BF16x3 banded
-Toeplitz products on tcgen05 with float32 accumulation. Not bit-identical to
-the float32 chain; checked against scipy.ndimage in float64 with the error
-bound written below (relative to the largest output magnitude)."""
+"""The split-precision tensor-core paths: algorithm="tensor" (TF32x3, the
+streaming TMA-fed kernel) and algorithm="tensor_bf16x3" (BF16x3). Neither is
+bit-identical to the float32 chain; both are checked against scipy.ndimage in
+float64 with the error bounds written below (max |err| relative to the
+largest output magnitude).
+
+Error model. TF32x3 loses up to about 1.1e-6 of the output scale per pass:
+the tensor core rounds its float32 accumulator toward zero at every MMA, a
+bias that grows with the slices summed into one accumulator (worst when a
+short axis folds all taps onto a few samples). The bound is therefore per
+pass: 2.2e-6 for a 2-D filter, 3.3e-6 for a 3-D one. BF16x3 is limited by
+its 16-bit operand splits: 1e-5 per pass."""
 
 import numpy as np
 import pytest
@@ -10,8 +18,9 @@ import torch
 
 pytestmark = pytest.mark.gpu
 
-# max |tensor - float64| / max |float64|
-REL_BOUND = 2e-5
+# max |tensor - float64| / max |float64|, per filter pass
+REL_BOUND_PER_PASS = {"tensor": 1.1e-6, "tensor_bf16x3": 1e-5}
+ALGOS = list(REL_BOUND_PER_PASS)
 MODES = ["reflect", "mirror", "nearest", "wrap", "constant"]
 
 
@@ -26,36 +35,97 @@ def ndi(cuda):
     return ndimage
 
 
-def _check(got, ref):
+def _check(got, ref, algo, passes=None):
     err = np.abs(got.astype(np.float64) - ref)
     scale = max(np.abs(ref).max(), 1e-30)
+    passes = got.ndim if passes is None else passes
     assert np.isfinite(got).all()
-    assert err.max() / scale < REL_BOUND, (err.max() / scale, err.mean() / scale)
+    bound = REL_BOUND_PER_PASS[algo] * passes
+    assert err.max() / scale < bound, (err.max() / scale, err.mean() / scale, bound)
 
 
+@pytest.mark.parametrize("algo", ALGOS)
 @pytest.mark.parametrize("shape", [(300, 257), (128, 64), (1, 700), (700, 3), (5, 130, 90)])
 @pytest.mark.parametrize("sigma", [4.0, 16.0])
 @pytest.mark.parametrize("mode", MODES)
-def test_tensor_gaussian(ndi, shape, sigma, mode):
+def test_tensor_gaussian(ndi, algo, shape, sigma, mode):
     x = np.random.default_rng(2).random(shape, dtype=np.float32)
-    got = ndi.gaussian_filter(dev(x), sigma, mode=mode, cval=0.5, algorithm="tensor")
+    got = ndi.gaussian_filter(dev(x), sigma, mode=mode, cval=0.5, algorithm=algo)
     ref = sndi.gaussian_filter(x.astype(np.float64), sigma, mode=mode, cval=0.5)
-    _check(got.cpu().numpy(), ref)
+    _check(got.cpu().numpy(), ref, algo)
 
 
+@pytest.mark.parametrize("algo", ALGOS)
 @pytest.mark.parametrize("axis", [0, 1])
 @pytest.mark.parametrize("K", [16, 63, 257, 385])
-def test_tensor_correlate_axes(ndi, axis, K):
+def test_tensor_correlate_axes(ndi, algo, axis, K):
     x = np.random.default_rng(K).standard_normal((517, 333)).astype(np.float32)
     w = np.random.default_rng(K + 1).random(K).astype(np.float32)
-    got = ndi.correlate1d(dev(x), w, axis, mode="nearest", algorithm="tensor")
+    got = ndi.correlate1d(dev(x), w, axis, mode="nearest", algorithm=algo)
     ref = sndi.correlate1d(x.astype(np.float64), w.astype(np.float64), axis, mode="nearest")
-    _check(got.cpu().numpy(), ref)
+    # with 385 taps over zero-mean data the partial sums outgrow the result,
+    # and the accumulator's rounding with them
+    _check(got.cpu().numpy(), ref, algo, passes=1.5 if K > 300 else 1)
 
 
-def test_tensor_uniform_and_derivative(ndi):
+@pytest.mark.parametrize("algo", ALGOS)
+def test_tensor_uniform_and_derivative(ndi, algo):
     x = np.random.default_rng(3).random((400, 380), dtype=np.float32)
+    got = ndi.uniform_filter(dev(x), 63, mode="nearest", algorithm=algo)
+    _check(got.cpu().numpy(), sndi.uniform_filter(x.astype(np.float64), 63, mode="nearest"), algo)
+    got = ndi.gaussian_filter(dev(x), 6.0, order=1, algorithm=algo)
+    _check(got.cpu().numpy(), sndi.gaussian_filter(x.astype(np.float64), 6.0, order=1), algo)
+
+
+# Shapes whose rows and lines are multiples of 4 take the TMA-fed staging of
+# the streaming kernel; many strips and blocks per CTA exercise the runs, the
+# accumulator ring and the stage ring.
+@pytest.mark.parametrize("shape", [(1024, 2048), (2048, 520), (3, 256, 264), (96, 4096)])
+@pytest.mark.parametrize("mode", ["nearest", "reflect", "constant"])
+def test_tf32x3_streaming_shapes(ndi, shape, mode):
+    x = np.random.default_rng(7).random(shape, dtype=np.float32) * 10 - 3
+    got = ndi.gaussian_filter(dev(x), 16.0, mode=mode, cval=1.5, algorithm="tensor")
+    ref = sndi.gaussian_filter(x.astype(np.float64), 16.0, mode=mode, cval=1.5)
+    _check(got.cpu().numpy(), ref, "tensor")
+
+
+@pytest.mark.parametrize("K", [17, 130, 258, 449])
+@pytest.mark.parametrize("origin", [-3, 0, 2])
+def test_tf32x3_taps_and_origins(ndi, K, origin):
+    # odd anchors exercise the zero taps that align the TMA window
+    x = np.random.default_rng(K).standard_normal((256, 1032)).astype(np.float32)
+    w = np.random.default_rng(K + 5).standard_normal(K).astype(np.float32)
+    if abs(origin) > K // 2 - (1 - K % 2):
+        pytest.skip("origin outside the filter")
+    for axis in (0, 1):
+        got = ndi.correlate1d(dev(x), w, axis, mode="mirror", origin=origin, algorithm="tensor")
+        ref = sndi.correlate1d(x.astype(np.float64), w.astype(np.float64), axis,
+                               mode="mirror", origin=origin)
+        _check(got.cpu().numpy(), ref, "tensor", passes=1)
+
+
+def test_tf32x3_rectangles_image(ndi):
+    # the precision workload's value distribution (uniform noise plus constant
+    # rectangles of values up to 10) on a 2048 x 2048 crop: within the 2e-6
+    # target for 2-D filters
+    from cucim_b200 import synthetic
+
+    x = synthetic.rectangles_image((2048, 2048), n_rect=16, seed=2)
+    for sigma in (16.0, 32.0):
+        got = ndi.gaussian_filter(dev(x), sigma, mode="nearest", algorithm="tensor")
+        ref = sndi.gaussian_filter(x.astype(np.float64), sigma, mode="nearest")
+        err = np.abs(got.cpu().numpy().astype(np.float64) - ref).max() / np.abs(ref).max()
+        assert err < 2e-6, (sigma, err)
     got = ndi.uniform_filter(dev(x), 63, mode="nearest", algorithm="tensor")
-    _check(got.cpu().numpy(), sndi.uniform_filter(x.astype(np.float64), 63, mode="nearest"))
-    got = ndi.gaussian_filter(dev(x), 6.0, order=1, algorithm="tensor")
-    _check(got.cpu().numpy(), sndi.gaussian_filter(x.astype(np.float64), 6.0, order=1))
+    ref = sndi.uniform_filter(x.astype(np.float64), 63, mode="nearest")
+    err = np.abs(got.cpu().numpy().astype(np.float64) - ref).max() / np.abs(ref).max()
+    assert err < 2e-6, err
+
+
+def test_tf32x3_device_status_clean(ndi):
+    from cucim_b200 import _lib
+
+    x = dev(np.random.default_rng(1).random((512, 512), dtype=np.float32))
+    ndi.gaussian_filter(x, 20.0, algorithm="tensor")
+    torch.cuda.synchronize()
+    assert _lib.lib.cimx_device_status(1) == 0
