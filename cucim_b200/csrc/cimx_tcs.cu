@@ -68,8 +68,10 @@ constexpr int kSlicesPerChunk = 4;  // tf32 MMA steps of 8 coordinates
 constexpr int kBPS = 16;            // slices per block step (128 outputs)
 constexpr int kMaxStages = 8;
 constexpr int kMaxSlots = 8;
-constexpr int kMmaWarp = 4, kTmaWarp = 5, kConvWarp0 = 6, kConvWarps = 8;
-constexpr int kThreads = 32 * (kConvWarp0 + kConvWarps);  // 448
+// warps 0-3 epilogue, 4-6 MMA issue (one thread each, on three different SM
+// sub-partitions), 7 TMA, 8-15 converters
+constexpr int kMmaWarp = 4, kIssuers = 3, kTmaWarp = 7, kConvWarp0 = 8, kConvWarps = 8;
+constexpr int kThreads = 32 * (kConvWarp0 + kConvWarps);  // 512
 constexpr int kConvThreads = 32 * kConvWarps;
 constexpr int kTcsMaxTaps = 452;  // taps after the alignment shift
 constexpr uint64_t kTcsWaitNs = 2000000000ull;
@@ -258,13 +260,13 @@ __global__ void __launch_bounds__(kThreads, 1)
     for (int i = 0; i < kMaxStages; ++i) {
       mbar_init(&full_tma[i], 1);
       mbar_init(&full_cv[i], kConvThreads);
-      mbar_init(&empty[i], 1);
+      mbar_init(&empty[i], kIssuers);
     }
     for (int i = 0; i < kMaxSlots; ++i) {
       mbar_init(&accf[i], 1);
       mbar_init(&acce[i], 128);
     }
-    mbar_init(done, 1);
+    mbar_init(done, kIssuers);
     *abort_flag = 0;
     mbar_fence_init();
   }
@@ -336,11 +338,15 @@ __global__ void __launch_bounds__(kThreads, 1)
       for (long long g = issued - a.NST < 0 ? 0 : issued - a.NST; g < issued; ++g)
         wait_bar(&full_tma[g % a.NST], (uint32_t)((g / a.NST) & 1), nullptr, nullptr);
     }
-  } else if (warp == kMmaWarp) {
+  } else if (warp >= kMmaWarp && warp < kMmaWarp + kIssuers) {
     // ------------------------------------------------------------ MMA
-    // A single thread issues every MMA; everything the issue loop needs is
-    // held in registers and advanced by additions.
+    // Three threads issue the MMAs, block gbi by thread gbi % 3, so that one
+    // block's MMAs, and its commit, come from one thread in order; every
+    // issuer commits every stage (the stage-free barrier counts three).
+    // Everything the issue loop needs is held in registers and advanced by
+    // additions.
     if (lane == 0) {
+      const uint32_t me = (uint32_t)(warp - kMmaWarp);
       const int nl = a.NL, nhh = a.NHH, nst = a.NST;
       const uint32_t nacc = (uint32_t)a.NACC, acc_mask = nacc - 1u;
       const int acc_shift = __ffs(a.NACC) - 1;
@@ -378,9 +384,10 @@ __global__ void __launch_bounds__(kThreads, 1)
           const int i_first = s0 < SB ? 0 : ((s0 - SB) >> 4) + 1;
           const int i_last = min(nb - 1, (s0 + kSlicesPerChunk - 1) >> 4);
           for (int i = i_first; i <= i_last; ++i) {
+            const uint32_t gbi = gb + (uint32_t)i;
+            if (gbi % kIssuers != me) continue;
             const int tt0 = s0 - kBPS * i;  // band slice of u = 0
             const int u_end = min(u_lim, SB - tt0);
-            const uint32_t gbi = gb + (uint32_t)i;
             const uint32_t slot = gbi & acc_mask;
             if (tt0 == 0 && gbi >= nacc) {
               if (!wait_bar(&acce[slot], ((gbi >> acc_shift) - 1u) & 1u, abort_flag, a.status)) {
