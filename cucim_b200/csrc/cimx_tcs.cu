@@ -13,10 +13,12 @@
 // MMAs accumulate hi*hi + hi*lo + lo*hi in float32 (TF32x3). The dropped
 // lo*lo term and the tf32 reading of lo leave a relative error per product
 // of about 2^-21. The tensor core rounds its float32 accumulator toward zero
-// at every MMA, a bias that grows with the number of MMAs into one
-// accumulator; hi*hi therefore accumulates alone (one MMA per slice) and the
-// two small cross terms in a second accumulator, the epilogue adding the two
-// with round-to-nearest. The result is not bit-identical to cuCIM's float32
+// as it aligns each product to the accumulator, a bias toward zero that
+// grows with the number of products summed into one accumulator at full
+// magnitude; hi*hi therefore accumulates alone, spread over NHH accumulators
+// (slice tt into accumulator tt mod NHH: 1 up to 64 taps, 2 up to 160, else
+// 3), and the two small cross terms go to one more accumulator; the epilogue
+// adds them with round-to-nearest. The result is not bit-identical to cuCIM's float32
 // chain.
 //
 // Streaming. A CTA owns a contiguous range of the flattened (strip, block)
@@ -86,7 +88,7 @@ struct TcsArgs {
   long long strips_per_o;  // strided: strips per outer index
   int K, anchor, mode;     // taps and anchor after the alignment shift
   int SB, BO, NL, NB, NACC, NST;  // BO = 128 outputs per block; NB = TMEM columns per slot
-  int NHH;                        // hi*hi accumulators per block (1, or 2 alternating)
+  int NHH;                        // hi*hi accumulators per block (1-3, by slice tt mod NHH)
   int use_tma, vec_out;
   uint32_t off_band_lo, off_stage0, stage_bytes, raw_bytes;
   uint32_t off_hi;  // offset of the hi tile in a stage (0: in place over the raw tile)
@@ -396,16 +398,16 @@ __global__ void __launch_bounds__(kThreads, 1)
               }
               tmem_fence_after();
             }
-            // slot: [hi*hi (one or two accumulators, by slice parity)][cross terms]
+            // slot: [hi*hi accumulators 0 .. NHH-1 (slice tt into tt mod NHH)][cross terms]
             const uint32_t d_slot = tmem + slot * slot_cols;
             const uint32_t d_x = d_slot + (uint32_t)(nhh * nl);
-            const uint32_t d_odd = d_slot + (nhh == 2 ? (uint32_t)nl : 0u);
             const uint64_t wh = wh0 - (uint64_t)(16 * tt0), wl = wl0 - (uint64_t)(16 * tt0);
+            int hsel = tt0 % nhh;
 #pragma unroll
-            for (int u = 0; u < kSlicesPerChunk; ++u) {
+            for (int u = 0; u < kSlicesPerChunk; ++u, hsel = (hsel + 1 == nhh) ? 0 : hsel + 1) {
               if (u < u_end) {
                 const int tt = tt0 + u;
-                const uint32_t d_hh = ((tt0 + u) & 1) ? d_odd : d_slot;
+                const uint32_t d_hh = d_slot + (uint32_t)(hsel * nl);
                 mma_tf32(d_hh, wh - 16 * u, xh + 2 * u, idesc, tt >= nhh ? 1u : 0u);  // hi * hi
                 mma_tf32(d_x, wh - 16 * u, xl + 2 * u, idesc, tt > 0 ? 1u : 0u);      // hi * lo
                 mma_tf32(d_x, wl - 16 * u, xh + 2 * u, idesc, 1u);                    // lo * hi
@@ -551,42 +553,43 @@ __global__ void __launch_bounds__(kThreads, 1)
         const long long lb = (r.b0 + i) * 128;
         const uint32_t tbase = tmem + ((uint32_t)(32 * warp) << 16) + slot * (uint32_t)a.NB;
         const long long l = lb + 32 * warp + lane;  // this thread's output
-        for (int q = 0; q < a.NL / 32; ++q) {
+        const int nq = a.NL / 32;
+        // per column group: read and sum the accumulators, release the slot
+        // after the last group's reads, then store
+        for (int q = 0; q < nq; ++q) {
+          const uint32_t col = tbase + 32 * q;
           float v[32], x[32];
-          tmem_ld32(tbase + 32 * q, v);
-          if (a.NHH == 2) {
-            tmem_ld32(tbase + a.NL + 32 * q, x);
+          tmem_ld32(col, v);
+          for (int h = 1; h <= a.NHH; ++h) {
+            tmem_ld32(col + h * a.NL, x);
 #pragma unroll
             for (int e = 0; e < 32; ++e) v[e] = __fadd_rn(v[e], x[e]);
           }
-          tmem_ld32(tbase + a.NHH * a.NL + 32 * q, x);
-#pragma unroll
-          for (int e = 0; e < 32; ++e) v[e] = __fadd_rn(v[e], x[e]);
+          if (q == nq - 1) {
+            tmem_fence_before();
+            mbar_arrive(&acce[slot]);
+          }
+          if (l >= a.L) continue;
           const long long n = r.n0 + 32 * q;  // first line of this column group
-          if (l < a.L) {
-            if (CONTIG) {
-              // lines are rows: a warp stores 32 consecutive outputs of a row
-              float* dst = a.out + n * a.L + l;
+          if (CONTIG) {
+            // lines are rows: a warp stores 32 consecutive outputs of a row
+            float* dst = a.out + n * a.L + l;
+#pragma unroll
+            for (int e = 0; e < 32; ++e)
+              if (n + e < a.rows) dst[e * a.L] = v[e];
+          } else {
+            float* dst = a.out + (r.o * a.L + l) * a.inner + n;
+            if (a.vec_out && n + 32 <= a.inner) {
+#pragma unroll
+              for (int e = 0; e < 32; e += 4)
+                *reinterpret_cast<float4*>(dst + e) = make_float4(v[e], v[e + 1], v[e + 2], v[e + 3]);
+            } else {
 #pragma unroll
               for (int e = 0; e < 32; ++e)
-                if (n + e < a.rows) dst[e * a.L] = v[e];
-            } else {
-              float* dst = a.out + (r.o * a.L + l) * a.inner + n;
-              if (a.vec_out && n + 32 <= a.inner) {
-#pragma unroll
-                for (int e = 0; e < 32; e += 4)
-                  *reinterpret_cast<float4*>(dst + e) =
-                      make_float4(v[e], v[e + 1], v[e + 2], v[e + 3]);
-              } else {
-#pragma unroll
-                for (int e = 0; e < 32; ++e)
-                  if (n + e < a.inner) dst[e] = v[e];
-              }
+                if (n + e < a.inner) dst[e] = v[e];
             }
           }
         }
-        tmem_fence_before();
-        mbar_arrive(&acce[slot]);
       }
       gb += (uint32_t)r.nb;
     }
@@ -619,17 +622,17 @@ bool plan_tcs(const PassDesc& d, TcsPlan& p) {
   p.K = d.K + p.delta;
   p.anchor = d.anchor + p.delta;
   if (p.K > kTcsMaxTaps) return false;
-  // hi*hi accumulates in one TMEM accumulator per block up to 160 taps; for
-  // longer filters it alternates between two by slice parity, halving the
-  // round-toward-zero bias of the tensor core's float32 accumulation.
-  p.NHH = p.K <= 160 ? 1 : 2;
+  // hi*hi accumulators per block: splitting the sum over NHH accumulators
+  // divides the round-toward-zero bias of the float32 accumulation by NHH
+  p.NHH = p.K <= 64 ? 1 : p.K <= 160 ? 2 : 3;
   p.BO = 128;
   p.SB = (p.BO + p.K - 1 + 7) / 8;
   const int need = (p.SB + 15) / 16;  // blocks a slice feeds at most
   // lines per strip: the widest whose ring of slots (a power of two, NB =
-  // (NHH + 1) NL TMEM columns each) leaves one slot of slack for the
-  // epilogue, else the widest that fits at all
-  for (int pass = 0; pass < 2; ++pass) {
+  // (NHH + 1) NL TMEM columns each) holds every block a slice feeds; wider
+  // strips make larger MMAs, which outweighs waiting for the epilogue when
+  // the ring has no spare slot (the epilogue frees a slot before its stores)
+  for (int pass = 1; pass < 2; ++pass) {
     for (int nl : {128, 64, 32}) {
       p.NL = nl;
       p.NB = (p.NHH + 1) * nl;
