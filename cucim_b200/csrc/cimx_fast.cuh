@@ -265,6 +265,10 @@ int launch_stream_td(const PassDesc& d, const float* w, int K, int anchor, bool 
 
 // ---------------------------------------------------------------- (b)
 
+// resident slab CTAs per SM asked of the compiler: four (64 registers a
+// thread) keep more tile loads in flight than three, which is what the
+// 74 registers a thread of the unconstrained build allowed
+constexpr int kSlabMinBlocks = 4;
 constexpr int kSlabTY = 32;    // output rows per tile
 constexpr int kSlabTX = 128;   // output columns per tile
 
@@ -424,7 +428,7 @@ __device__ __forceinline__ float staged_value(const T* in, long long gy, long lo
 }
 
 template <class T, class D, int KB, bool TMA>
-__global__ void __launch_bounds__(256) k_slab(const __grid_constant__ CUtensorMap map,
+__global__ void __launch_bounds__(256, kSlabMinBlocks) k_slab(const __grid_constant__ CUtensorMap map,
                                                const SlabArgs a) {
   using G = Geom<T, KB>;
   extern __shared__ __align__(128) unsigned char smem[];
