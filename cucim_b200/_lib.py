@@ -53,6 +53,18 @@ class CimxArray(ctypes.Structure):
     ]
 
 
+class CimxBatchTile(ctypes.Structure):
+    _fields_ = [
+        ("rgb", ctypes.c_void_p),
+        ("out", ctypes.c_void_p),
+        ("height", ctypes.c_int32),
+        ("width", ctypes.c_int32),
+        ("ntaps", ctypes.c_int32),
+        ("taps_offset", ctypes.c_int32),
+        ("first_block", ctypes.c_int64),
+    ]
+
+
 class CimxPass(ctypes.Structure):
     _fields_ = [
         ("axis", ctypes.c_int32),
@@ -93,6 +105,11 @@ _sigs = {
     "cimx_rgb2gray": ([_A, _A, ctypes.c_void_p], ctypes.c_int),
     "cimx_convert": ([_A, _A, ctypes.c_int, ctypes.c_void_p], ctypes.c_int),
     "cimx_gradient_fd": ([_A, _A, ctypes.c_int, ctypes.c_void_p], ctypes.c_int),
+    "cimx_batch_gray_gauss_sobel": (
+        [ctypes.c_void_p, ctypes.c_int, ctypes.c_longlong, ctypes.c_void_p, ctypes.c_int,
+         _P(ctypes.c_float), _P(ctypes.c_float), ctypes.c_void_p],
+        ctypes.c_int,
+    ),
     "cimx_frangi_accumulate": (
         [_A, ctypes.c_int, _A, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int,
          ctypes.c_void_p, ctypes.c_void_p],

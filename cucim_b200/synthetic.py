@@ -64,6 +64,26 @@ def rgb_tiles(n_tiles=4096, side_range=(64, 1024), seed=3, sigma_range=(0.5, 8.0
     return tiles, sigmas
 
 
+def rgb_tiles_device(device, n_tiles=4096, side_range=(64, 1024), seed=3, sigma_range=(0.5, 8.0)):
+    """rgb_tiles generated on the device: the same tile sides and sigmas as
+    rgb_tiles (numpy, seed 3), pixel values from the same 3-component mixture
+    (means 60 / 150 / 220, sd 20, equal weights, rounded, clipped to
+    [0, 255]) drawn with a seeded torch generator."""
+    import torch
+
+    rng = np.random.default_rng(seed)
+    sides = [rng.integers(side_range[0], side_range[1] + 1, 2) for _ in range(n_tiles)]
+    sigmas = [float(rng.uniform(*sigma_range)) for _ in range(n_tiles)]
+    g = torch.Generator(device=device).manual_seed(seed)
+    means = torch.tensor([60.0, 150.0, 220.0], device=device)
+    tiles = []
+    for h, w in sides:
+        comp = torch.randint(0, 3, (int(h), int(w), 3), generator=g, device=device)
+        vals = torch.randn((int(h), int(w), 3), generator=g, device=device) * 20.0 + means[comp]
+        tiles.append(vals.round_().clamp_(0, 255).to(torch.uint8))
+    return tiles, sigmas
+
+
 def segments_volume(shape=(256, 256, 256), n_segments=200, seed=4,
                     length_range=(20, 120), radius_range=(1.0, 4.0)):
     rng = np.random.default_rng(seed)

@@ -206,6 +206,34 @@ CIMX_API int cimx_frangi_accumulate(const CimxArray* eigs, int ndim, const CimxA
                                     double alpha, double beta, double gamma, int first,
                                     void* gamma_state, void* stream);
 
+/* One tile of a batch for cimx_batch_gray_gauss_sobel. */
+typedef struct CimxBatchTile {
+  const uint8_t* rgb;   /* device: height x width x 3 uint8, C-contiguous */
+  float* out;           /* device: height x width float32, C-contiguous */
+  int32_t height, width;
+  int32_t ntaps;        /* gaussian taps of this tile (odd, <= max_taps) */
+  int32_t taps_offset;  /* index of the tile's first tap in `taps` */
+  int64_t first_block;  /* index of the tile's first 64 x 64 output block; tiles in
+                           ascending order, the first at 0 */
+} CimxBatchTile;
+
+/* For every tile of a batch: rgb2gray (color/colorconv.py:1038-1095 with the
+ * uint8 -> float32 scaling of util/dtype.py:360-361), a gaussian with the
+ * tile's own float32 taps and mode 'nearest' (skimage.filters.gaussian,
+ * _shared/filters.py:21-166), then the sobel gradient magnitude with mode
+ * 'reflect' (filters/edges.py:148-306: edge taps `edge_taps` along one axis,
+ * `smooth_taps` along the other, both as correlation taps after the
+ * convolution flip), float32 out — one persistent launch over the tiles'
+ * 64 x 64 output blocks (`nblocks` in all). Results are bit-identical to the
+ * three per-tile calls. `tiles` and `taps` are device memory prepared by the
+ * caller, so the launch can be captured in a CUDA graph and replayed;
+ * `edge_taps` and `smooth_taps` are 3 host floats read at the call.
+ * No counterpart in cuCIM, which runs the three functions per tile. */
+CIMX_API int cimx_batch_gray_gauss_sobel(const CimxBatchTile* tiles, int ntiles,
+                                         long long nblocks, const float* taps, int max_taps,
+                                         const float* edge_taps, const float* smooth_taps,
+                                         void* stream);
+
 #ifdef __cplusplus
 }
 #endif
