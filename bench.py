@@ -19,6 +19,11 @@ largest output magnitude against a float64 scipy.ndimage reference on a
 2048 x 2048 crop (4.2 Mpx; the full image would take minutes on the CPU).
 The 256 MiB image alone is above L2; every timed repetition reads it from HBM.
 
+Frangi (reported in `frangi`): skimage.filters.frangi(sigmas=1..5,
+alpha=beta=0.5, gamma=None, black_ridges=False) on the 256^3 float32
+segments volume (seed 4), with the plain float32 passes and with
+algorithm="tensor", and the largest difference between the two.
+
 Batched tiles (reported in `batched_tiles`): 4096 uint8 RGB tiles with
 sides drawn from 64..1024 (seed 3; about 1.2 Gpx), each filtered by
 rgb2gray -> gaussian(its own sigma in [0.5, 8]) -> sobel magnitude, once as
@@ -66,6 +71,7 @@ def parse():
                    help="run only the precision path and the batched tiles (for profiling)")
     p.add_argument("--no-tiles", action="store_true", help="skip the batched-tiles report")
     p.add_argument("--tiles", type=int, default=4096, help="tiles in the batched-tiles report")
+    p.add_argument("--no-frangi", action="store_true", help="skip the frangi report")
     return p.parse_args()
 
 
@@ -259,9 +265,13 @@ def run_ours(args, rank, world, local_rank):
     if rank == 0 and not args.no_tiles:
         torch.cuda.empty_cache()
         tiles = run_tiles(torch, dev, n_tiles=args.tiles)
+    fr = None
+    if rank == 0 and not args.no_frangi:
+        torch.cuda.empty_cache()
+        fr = run_frangi(torch, dev)
 
     return {"value": value, "ms": ms, "nvox": nvox, "kernels": kres, "clocks": clk.summary(),
-            "e2e": e2e, "x": x_host, "precision": prec, "tiles": tiles}
+            "e2e": e2e, "x": x_host, "precision": prec, "tiles": tiles, "frangi": fr}
 
 
 def run_e2e(ndi, torch, x, shape, douts, args, world):
@@ -399,6 +409,35 @@ def run_tiles(torch, dev, reps=3, check=64, n_tiles=4096):
             "bit_identical": bool(same), "tiles_compared": len(range(0, len(tiles), step))}
 
 
+# --------------------------------------------------------------- frangi
+
+def run_frangi(torch, dev, reps=3):
+    """Multi-scale frangi (sigmas 1..5, alpha = beta = 0.5, automatic gamma,
+    black_ridges=False) on the seed-4 segments volume: plain float32 passes
+    against algorithm="tensor", and the largest difference between the two
+    relative to the largest output."""
+    from cucim_b200 import synthetic
+    from cucim_b200.skimage import filters
+
+    vol = torch.as_tensor(synthetic.segments_volume((256, 256, 256), seed=4)).to(dev)
+    kw = dict(sigmas=range(1, 6), alpha=0.5, beta=0.5, gamma=None, black_ridges=False)
+    res = {}
+    outs = {}
+    for algo, key in ((None, "plain_f32"), ("tensor", "tensor_tf32x3")):
+        f = lambda: filters.frangi(vol, algorithm=algo, **kw)  # noqa: E731
+        ms = time_kernel(f, reps, torch)
+        outs[key] = f()
+        res[key] = {"ms": ms, "gvox_s": vol.numel() / (ms * 1e-3) / 1e9}
+    p, t = outs["plain_f32"].double(), outs["tensor_tf32x3"].double()
+    scale = float(p.abs().max())
+    res["speedup"] = res["plain_f32"]["ms"] / res["tensor_tf32x3"]["ms"]
+    res["tensor_vs_plain_max_rel"] = float((t - p).abs().max()) / scale
+    res["tensor_vs_plain_mean_rel"] = float((t - p).abs().mean()) / scale
+    return {"workload": "float32 256^3 segments volume (seed 4), frangi sigmas 1..5, "
+                        "27 Gaussian-derivative passes per sigma (taps 143, 23, 35, 47, 57)",
+            **res}
+
+
 # ------------------------------------------------------------- CPU leg
 
 def cpu_baseline(x_host, slab_z=16, threads=None):
@@ -488,6 +527,8 @@ def main():
                     tf32_peak=_peaks().get("bf16_tflops", 1590.0) / 2)
             if not args.no_tiles:
                 out["batched_tiles"] = run_tiles(torch, dev, n_tiles=args.tiles)
+            if not args.no_frangi:
+                out["frangi"] = run_frangi(torch, dev)
             print(json.dumps(out))
         return
     if world > 1:
@@ -516,7 +557,7 @@ def main():
             "roofline": roof, "kernels": res["kernels"], "cpu_baseline": cpu,
             "e2e": res["e2e"], "gpu_launches": LAUNCHES_PER_STEP * args.steps,
             "clocks": res["clocks"], "precision_path": res["precision"],
-            "batched_tiles": res["tiles"],
+            "batched_tiles": res["tiles"], "frangi": res["frangi"],
         }
         print(json.dumps(line))
     if world > 1:

@@ -667,9 +667,232 @@ int launch_slab_kb(SlabArgs& a, cudaStream_t st) {
   return cuda_fail(cudaGetLastError(), "slab launch");
 }
 
+
+// ---------------------------------------------------------------- (c)
+// Row streaming: the fused (y, x) passes of a slab when the rows are short
+// enough for one CTA (X % 4 == 0, X / 4 threads: X <= 4096, or 2048 for
+// K >= 9) and both passes
+// have the same compile-time length K in {3, 5, 9, 17} without skipped taps.
+// A CTA walks a chunk of rows of one slab: every thread prefetches its 4
+// columns of the row DEPTH steps ahead with cp.async (no boundary columns:
+// every load is an aligned vector inside the row), keeps K rows in a
+// register ring, runs the y chain, and writes the row — rounded through D —
+// to one of two shared row buffers; after one barrier it runs the x chain
+// for its 4 outputs from the buffer. Each buffer has K - 1 halo slots on
+// both sides holding the intermediate at the mapped column (written each row
+// by the thread that owns that column, from a bit mask computed once) or the
+// x fill value in constant mode: that is how cuCIM's second pass sees the
+// first pass's output beyond the row ends. The arithmetic, tap order and
+// rounding are those of k_slab.
+template <int K>
+struct RowArgs {
+  const void* in;
+  void* out;
+  long long B, Y, X;
+  long long chunk;
+  int ay, ax, my, mx;
+  double cval_y, cval_x;  // fill values, rounded in the kernel as k_slab rounds them
+  int cin_y, cin_x, dt_y, dt_x;
+  float wy[K], wx[K];
+};
+
+template <int K> constexpr int row_depth() { return K * ((8 + K - 1) / K); }
+// threads per CTA at most (one per 4 columns): long rings need more registers
+template <int K> constexpr int row_max_threads() { return K >= 9 ? 512 : 1024; }
+
+// row buffer (floats): RP halo slots, 4 * nthreads columns, RP halo slots, 4
+// spare; RP = K - 1 rounded up to 4 keeps every float4 of the row 16-byte
+// aligned. The prefetch region before the buffers is rounded up to 16 bytes.
+template <int K> constexpr int row_pad() { return (K - 1 + 3) / 4 * 4; }
+template <int K> constexpr int row_buf(int nthreads) { return 4 * nthreads + 2 * row_pad<K>() + 4; }
+template <class T, int K>
+constexpr size_t row_pre_bytes(int nthreads) {
+  return ((size_t)row_depth<K>() * nthreads * 4 * sizeof(T) + 15) / 16 * 16;
+}
+template <class T, int K>
+constexpr size_t row_smem(int nthreads) {
+  return row_pre_bytes<T, K>(nthreads) + 2 * (size_t)row_buf<K>(nthreads) * 4;
+}
+
+template <class T, class D, int K>
+__global__ void __launch_bounds__(row_max_threads<K>()) k_rowstream(const RowArgs<K> a) {
+  constexpr int DEPTH = row_depth<K>();
+  extern __shared__ __align__(16) unsigned char sm_rows[];
+  const int NT = blockDim.x;
+  const int t = threadIdx.x;
+  T* pre = reinterpret_cast<T*>(sm_rows) + t * 4;  // prefetch slot d at pre + d * NT * 4
+  // row buffers; column c of buffer j at R0 + j * RS + c (RP halo slots before)
+  float* R0 = reinterpret_cast<float*>(sm_rows + row_pre_bytes<T, K>(NT)) + row_pad<K>();
+  const int RS = row_buf<K>(NT);
+  const long long X = a.X, Y = a.Y;
+  const float cy = fill_value<float>(a.cval_y, a.cin_y, a.dt_y);
+  const float cx = fill_value<float>(a.cval_x, a.cin_x, a.dt_x);
+  const long long c0 = 4LL * t;  // this thread's first column
+  const long long l0 = (long long)blockIdx.x * a.chunk;
+  const long long l1 = min(l0 + a.chunk, Y);
+  const long long n = l1 - l0;
+  // halo slots: h = -ax .. -1 (bits 0 .. ax-1) and X .. X + K - 2 - ax (bits
+  // ax ..); this thread fills the slots whose mapped column is one of its own
+  const int nleft = a.ax, nhalo = K - 1;
+  auto halo_col = [&](int i) { return i < nleft ? i - nleft : static_cast<int>(X) + (i - nleft); };
+  uint32_t own = 0;
+  for (int i = 0; i < nhalo; ++i) {
+    const int m = map_coord32(halo_col(i), static_cast<int>(X), a.mx);
+    if (m >= 0 && m >= c0 && m < c0 + 4) own |= 1u << i;
+  }
+  if (a.mx == CIMX_MODE_CONSTANT) {
+    // constant mode: the halo holds the fill value for good
+    for (int i = t; i < 2 * nhalo; i += NT)
+      R0[(i / nhalo) * RS + halo_col(i % nhalo)] = cx;
+  }
+
+  for (long long b = blockIdx.y; b < a.B; b += gridDim.y) {
+    const T* in = static_cast<const T*>(a.in) + b * Y * X + c0;
+    D* out = static_cast<D*>(a.out) + b * Y * X + c0;
+    auto mapped = [&](long long r) -> long long {
+      return (r < 0 || r >= Y) ? map_coord(r, Y, a.my) : r;
+    };
+    auto load_row = [&](float (&v)[4], long long r) {
+      const long long m = mapped(r);
+      if (m < 0) v[0] = v[1] = v[2] = v[3] = cy;
+      else load4<T>(in + m * X, v);
+    };
+    auto row_of_step = [&](long long s) { return l0 + s - a.ay + K - 1; };
+    auto issue = [&](int slot, long long s) {
+      const long long m = mapped(row_of_step(s));
+      if (m >= 0) cp_async_vec4<T>(pre + (size_t)slot * NT * 4, in + m * X);
+      cp_commit();
+    };
+    float win[K][4];
+#pragma unroll
+    for (int k = 0; k < K - 1; ++k) load_row(win[k], l0 - a.ay + k);
+#pragma unroll
+    for (int d = 0; d < DEPTH - 1; ++d) issue(d, d);
+
+    for (long long s0 = 0; s0 < n; s0 += DEPTH) {
+#pragma unroll
+      for (int u = 0; u < DEPTH; ++u) {
+        const long long s = s0 + u;
+        if (s < n) {  // the same for every thread of the CTA
+          issue((u + DEPTH - 1) % DEPTH, s + DEPTH - 1);
+          cp_wait<DEPTH - 1>();
+          float* v = win[(u + K - 1) % K];
+          const long long m = mapped(row_of_step(s));
+          if (m < 0) {
+            v[0] = v[1] = v[2] = v[3] = cy;
+          } else {
+            const typename Vec4<T>::type q =
+                *reinterpret_cast<const typename Vec4<T>::type*>(pre + (size_t)u * NT * 4);
+            v[0] = static_cast<float>(q.x);
+            v[1] = static_cast<float>(q.y);
+            v[2] = static_cast<float>(q.z);
+            v[3] = static_cast<float>(q.w);
+          }
+          // y chain, rounded through D into this step's row buffer
+          float acc[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+          for (int k = 0; k < K; ++k)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) acc[e] = fmaf(win[(u + k) % K][e], a.wy[k], acc[e]);
+          float* R = R0 + (s & 1) * RS;
+          float iv[4];
+#pragma unroll
+          for (int e = 0; e < 4; ++e) iv[e] = static_cast<float>(out_cast<D>(acc[e]));
+          *reinterpret_cast<float4*>(R + c0) = make_float4(iv[0], iv[1], iv[2], iv[3]);
+          for (uint32_t bits = own; bits; bits &= bits - 1) {
+            const int i = __ffs(bits) - 1;
+            const int h = halo_col(i);
+            const int e = map_coord32(h, static_cast<int>(X), a.mx) - static_cast<int>(c0);
+            R[h] = e == 0 ? iv[0] : e == 1 ? iv[1] : e == 2 ? iv[2] : iv[3];
+          }
+          __syncthreads();
+          // x chain for outputs c0 .. c0 + 3
+          float xo[4] = {0.f, 0.f, 0.f, 0.f};
+          float rv[K + 3];
+#pragma unroll
+          for (int j = 0; j < K + 3; ++j) rv[j] = R[c0 - a.ax + j];
+#pragma unroll
+          for (int k = 0; k < K; ++k)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) xo[e] = fmaf(rv[e + k], a.wx[k], xo[e]);
+          store4<D>(out + (l0 + s) * X, xo[0], xo[1], xo[2], xo[3]);
+        }
+      }
+    }
+    cp_wait<0>();
+    __syncthreads();  // the row buffers are reused by the next slab
+  }
+}
+
+template <class T, class D, int K>
+int launch_rowstream_k(const SlabArgs& s, cudaStream_t st) {
+  RowArgs<K> a{};
+  a.in = s.in;
+  a.out = s.out;
+  a.B = s.B;
+  a.Y = s.Y;
+  a.X = s.X;
+  a.ay = s.py.anchor;
+  a.ax = s.px.anchor;
+  a.my = s.py.mode;
+  a.mx = s.px.mode;
+  a.cval_y = s.py.cval;
+  a.cval_x = s.px.cval;
+  a.cin_y = s.py.cval_as_input;
+  a.cin_x = s.px.cval_as_input;
+  a.dt_y = s.py.dt;
+  a.dt_x = s.px.dt;
+  for (int k = 0; k < K; ++k) {
+    a.wy[k] = s.py.w[k];
+    a.wx[k] = s.px.w[k];
+  }
+  const int nt = static_cast<int>(s.X / 4);
+  const size_t smem = row_smem<T, K>(nt);
+  static std::once_flag once;
+  std::call_once(once, [] {
+    cudaFuncSetAttribute(k_rowstream<T, D, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         kMaxSmem);
+  });
+  // rows per CTA: enough CTAs to fill the GPU a few times over
+  long long chunk = 128;
+  while (chunk > 16 && s.B * ((s.Y + chunk - 1) / chunk) < 148LL * 4) chunk /= 2;
+  a.chunk = chunk;
+  const long long nchunks = (s.Y + chunk - 1) / chunk;
+  if (nchunks > 0x7fffffffLL) return CIMX_FUSED_DECLINED;
+  const dim3 grid((unsigned)nchunks, (unsigned)std::min<long long>(s.B, 65535));
+  k_rowstream<T, D, K><<<grid, nt, smem, st>>>(a);
+  return cuda_fail(cudaGetLastError(), "row stream launch");
+}
+
+template <class T, class D>
+bool rowstream_fits(const SlabArgs& s) {
+  if (!s.has_x || !s.has_y || s.py.skip || s.px.skip || s.py.K != s.px.K) return false;
+  if (s.X % 4 != 0 || s.X < 4 || s.Y < 1) return false;
+  // measured: faster than the slab kernel for 3 and 5 taps (3.9 / 3.1 TB/s on
+  // a 512 x 1024 x 1024 float32 stack), slower for 9 and 17
+  const int K = s.py.K;
+  if (K != 3 && K != 5) return false;
+  if (s.X / 4 > (K >= 9 ? row_max_threads<9>() : row_max_threads<3>())) return false;
+  const size_t smem = K == 3 ? row_smem<T, 3>(s.X / 4)
+                      : K == 5 ? row_smem<T, 5>(s.X / 4)
+                      : K == 9 ? row_smem<T, 9>(s.X / 4) : row_smem<T, 17>(s.X / 4);
+  return smem <= (size_t)kMaxSmem;
+}
+
+template <class T, class D>
+int launch_rowstream_td(const SlabArgs& s, cudaStream_t st) {
+  switch (s.py.K) {
+    case 3: return launch_rowstream_k<T, D, 3>(s, st);
+    case 5: return launch_rowstream_k<T, D, 5>(s, st);
+    case 9: return launch_rowstream_k<T, D, 9>(s, st);
+    default: return launch_rowstream_k<T, D, 17>(s, st);
+  }
+}
+
 template <class T, class D>
 int launch_slab_td(SlabArgs& a, cudaStream_t st) {
   if (!a.has_y) return CIMX_FUSED_DECLINED;
+  if (rowstream_fits<T, D>(a)) return launch_rowstream_td<T, D>(a, st);
   const int k8 = std::max(a.py.K8, a.has_x ? a.px.K8 : 0);
   if (k8 <= 8) return launch_slab_kb<T, D, 8>(a, st);
   if (k8 <= 16) return launch_slab_kb<T, D, 16>(a, st);

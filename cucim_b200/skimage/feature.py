@@ -22,10 +22,13 @@ def _as_float_image(image):
     return _u.astype(image, fdt)
 
 
-def _hessian_matrix_with_gaussian(image, sigma=1, mode="reflect", cval=0, order="rc"):
+def _hessian_matrix_with_gaussian(image, sigma=1, mode="reflect", cval=0, order="rc", *,
+                                  algorithm=None):
     """corner.py:161-254: Gaussian-derivative Hessian. sigma is scaled by
     1/sqrt(2) for each of the two first-derivative passes; truncate is 8 when
-    every sigma exceeds 1 and 100 otherwise."""
+    every sigma exceeds 1 and 100 otherwise. `algorithm` is passed to
+    gaussian_filter ("tensor" runs the float32 passes with 16 taps or more on
+    the tensor cores; an addition of this library)."""
     image = _as_float_image(image)
     x = _arrays.as_tensor(image)
     ndim = x.dim()
@@ -42,7 +45,7 @@ def _hessian_matrix_with_gaussian(image, sigma=1, mode="reflect", cval=0, order=
 
     def g(img, o):
         return ndi.gaussian_filter(img, sigma_scaled, order=o, mode=mode, cval=cval,
-                                   truncate=truncate)
+                                   truncate=truncate, algorithm=algorithm)
 
     gradients = [g(image, orders[d]) for d in range(ndim)]
     axes = range(ndim)

@@ -111,9 +111,13 @@ def prewitt(image, mask=None, *, axis=None, mode="reflect", cval=0.0):
 
 
 def frangi(image, sigmas=range(1, 10, 2), scale_range=None, scale_step=None, alpha=0.5,
-           beta=0.5, gamma=None, black_ridges=True, mode="reflect", cval=0):
+           beta=0.5, gamma=None, black_ridges=True, mode="reflect", cval=0, *,
+           algorithm=None):
     """ridges.py:322-476. The automatic gamma (half the largest Hessian norm
-    of the first scale) stays on the device: no host synchronisation."""
+    of the first scale) stays on the device: no host synchronisation.
+    `algorithm="tensor"` (an addition of this library) runs the Hessian's
+    Gaussian-derivative passes with 16 taps or more on the tensor cores
+    (TF32x3); the default is cuCIM's float32 arithmetic."""
     if scale_range is not None and scale_step is not None:
         sigmas = np.arange(scale_range[0], scale_range[1], scale_step)
     x = _arrays.as_tensor(image)
@@ -131,7 +135,7 @@ def frangi(image, sigmas=range(1, 10, 2), scale_range=None, scale_step=None, alp
     g = float("nan") if gamma is None else float(gamma)
     a_out = _arrays.to_cimx(out)
     for i, sigma in enumerate(sigmas):
-        H = _hessian_matrix_with_gaussian(image, sigma, mode=mode, cval=cval)
+        H = _hessian_matrix_with_gaussian(image, sigma, mode=mode, cval=cval, algorithm=algorithm)
         ev = _arrays.as_tensor(symmetric_compute_eigenvalues(H, sort="ascending", abs_sort=True))
         eigs = (_lib.CimxArray * ndim)(*[_arrays.to_cimx(ev[k]) for k in range(ndim)])
         rc = _lib.lib.cimx_frangi_accumulate(eigs, ndim, ctypes.byref(a_out), float(alpha),
