@@ -769,6 +769,36 @@ __global__ void __launch_bounds__(row_max_threads<K>()) k_rowstream(const RowArg
 #pragma unroll
     for (int d = 0; d < DEPTH - 1; ++d) issue(d, d);
 
+    // x chain of row r (its y row is complete in buffer r & 1), stored
+    const bool x_aligned = (a.ax & 3) == 0;
+    auto x_row = [&](long long r) {
+      const float* R = R0 + (r & 1) * RS + (c0 - a.ax);
+      float rv[(K + 3 + 3) / 4 * 4];
+      if (x_aligned) {
+#pragma unroll
+        for (int q = 0; q < (K + 3 + 3) / 4; ++q) {
+          const float4 f = *reinterpret_cast<const float4*>(R + 4 * q);
+          rv[4 * q] = f.x;
+          rv[4 * q + 1] = f.y;
+          rv[4 * q + 2] = f.z;
+          rv[4 * q + 3] = f.w;
+        }
+      } else {
+#pragma unroll
+        for (int j = 0; j < K + 3; ++j) rv[j] = R[j];
+      }
+      float xo[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+      for (int k = 0; k < K; ++k)
+#pragma unroll
+        for (int e = 0; e < 4; ++e) xo[e] = fmaf(rv[e + k], a.wx[k], xo[e]);
+      store4<D>(out + (l0 + r) * X, xo[0], xo[1], xo[2], xo[3]);
+    };
+
+    // step s: the y chain of row s into buffer s & 1, then the x chain of
+    // row s - 1 (independent work the compiler interleaves), then one
+    // barrier. A buffer is rewritten two steps after it was read, and every
+    // thread has passed the barrier in between.
     for (long long s0 = 0; s0 < n; s0 += DEPTH) {
 #pragma unroll
       for (int u = 0; u < DEPTH; ++u) {
@@ -805,20 +835,12 @@ __global__ void __launch_bounds__(row_max_threads<K>()) k_rowstream(const RowArg
             const int e = map_coord32(h, static_cast<int>(X), a.mx) - static_cast<int>(c0);
             R[h] = e == 0 ? iv[0] : e == 1 ? iv[1] : e == 2 ? iv[2] : iv[3];
           }
+          if (s > 0) x_row(s - 1);
           __syncthreads();
-          // x chain for outputs c0 .. c0 + 3
-          float xo[4] = {0.f, 0.f, 0.f, 0.f};
-          float rv[K + 3];
-#pragma unroll
-          for (int j = 0; j < K + 3; ++j) rv[j] = R[c0 - a.ax + j];
-#pragma unroll
-          for (int k = 0; k < K; ++k)
-#pragma unroll
-            for (int e = 0; e < 4; ++e) xo[e] = fmaf(rv[e + k], a.wx[k], xo[e]);
-          store4<D>(out + (l0 + s) * X, xo[0], xo[1], xo[2], xo[3]);
         }
       }
     }
+    if (n > 0) x_row(n - 1);
     cp_wait<0>();
     __syncthreads();  // the row buffers are reused by the next slab
   }
@@ -868,8 +890,10 @@ template <class T, class D>
 bool rowstream_fits(const SlabArgs& s) {
   if (!s.has_x || !s.has_y || s.py.skip || s.px.skip || s.py.K != s.px.K) return false;
   if (s.X % 4 != 0 || s.X < 4 || s.Y < 1) return false;
-  // measured: faster than the slab kernel for 3 and 5 taps (3.9 / 3.1 TB/s on
-  // a 512 x 1024 x 1024 float32 stack), slower for 9 and 17
+  // measured on a 512 x 1024 x 1024 float32 stack: 4.0 / 3.1 TB/s for 3 / 5
+  // taps, faster than the slab kernel; 9 and 17 taps run at 1.7 / 0.94 TB/s,
+  // below the slab's 2.4 / 1.9 (16 warps per SM cannot hide the dependent
+  // chains between row barriers)
   const int K = s.py.K;
   if (K != 3 && K != 5) return false;
   if (s.X / 4 > (K >= 9 ? row_max_threads<9>() : row_max_threads<3>())) return false;
