@@ -672,7 +672,8 @@ int launch_slab_kb(SlabArgs& a, cudaStream_t st) {
 // Row streaming: the fused (y, x) passes of a slab when the rows are short
 // enough for one CTA (X % 4 == 0, X / 4 threads: X <= 4096, or 2048 for
 // K >= 9) and both passes
-// have the same compile-time length K in {3, 5, 9, 17} without skipped taps.
+// have the same compile-time length K in {3, 5} (zero taps skipped when the
+// pass says so).
 // A CTA walks a chunk of rows of one slab: every thread prefetches its 4
 // columns of the row DEPTH steps ahead with cp.async (no boundary columns:
 // every load is an aligned vector inside the row), keeps K rows in a
@@ -693,6 +694,7 @@ struct RowArgs {
   int ay, ax, my, mx;
   double cval_y, cval_x;  // fill values, rounded in the kernel as k_slab rounds them
   int cin_y, cin_x, dt_y, dt_x;
+  uint32_t act_y, act_x;  // bit k: tap k takes part in the chain (zero taps skipped)
   float wy[K], wx[K];
 };
 
@@ -790,8 +792,9 @@ __global__ void __launch_bounds__(row_max_threads<K>()) k_rowstream(const RowArg
       float xo[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
       for (int k = 0; k < K; ++k)
+        if ((a.act_x >> k) & 1u)
 #pragma unroll
-        for (int e = 0; e < 4; ++e) xo[e] = fmaf(rv[e + k], a.wx[k], xo[e]);
+          for (int e = 0; e < 4; ++e) xo[e] = fmaf(rv[e + k], a.wx[k], xo[e]);
       store4<D>(out + (l0 + r) * X, xo[0], xo[1], xo[2], xo[3]);
     };
 
@@ -822,8 +825,9 @@ __global__ void __launch_bounds__(row_max_threads<K>()) k_rowstream(const RowArg
           float acc[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
           for (int k = 0; k < K; ++k)
+            if ((a.act_y >> k) & 1u)
 #pragma unroll
-            for (int e = 0; e < 4; ++e) acc[e] = fmaf(win[(u + k) % K][e], a.wy[k], acc[e]);
+              for (int e = 0; e < 4; ++e) acc[e] = fmaf(win[(u + k) % K][e], a.wy[k], acc[e]);
           float* R = R0 + (s & 1) * RS;
           float iv[4];
 #pragma unroll
@@ -864,9 +868,13 @@ int launch_rowstream_k(const SlabArgs& s, cudaStream_t st) {
   a.cin_x = s.px.cval_as_input;
   a.dt_y = s.py.dt;
   a.dt_x = s.px.dt;
+  a.act_y = a.act_x = 0;
   for (int k = 0; k < K; ++k) {
     a.wy[k] = s.py.w[k];
     a.wx[k] = s.px.w[k];
+    // with skipping, a zero tap leaves the chain (k_slab's chain2 does the same)
+    if (!(s.py.skip && s.py.w[k] == 0.f)) a.act_y |= 1u << k;
+    if (!(s.px.skip && s.px.w[k] == 0.f)) a.act_x |= 1u << k;
   }
   const int nt = static_cast<int>(s.X / 4);
   const size_t smem = row_smem<T, K>(nt);
@@ -888,7 +896,7 @@ int launch_rowstream_k(const SlabArgs& s, cudaStream_t st) {
 
 template <class T, class D>
 bool rowstream_fits(const SlabArgs& s) {
-  if (!s.has_x || !s.has_y || s.py.skip || s.px.skip || s.py.K != s.px.K) return false;
+  if (!s.has_x || !s.has_y || s.py.K != s.px.K) return false;
   if (s.X % 4 != 0 || s.X < 4 || s.Y < 1) return false;
   // measured on a 512 x 1024 x 1024 float32 stack: 4.0 / 3.1 TB/s for 3 / 5
   // taps, faster than the slab kernel; 9 and 17 taps run at 1.7 / 0.94 TB/s,
