@@ -58,7 +58,24 @@ __device__ __forceinline__ void tap_loop(W (&acc)[P], const W* taps, int K, At a
   W win[2 * P];
 #pragma unroll
   for (int j = 0; j < P; ++j) win[j] = at(j);
-  for (int k0 = 0; k0 < K; k0 += P) {
+  int k0 = 0;
+  // full chunks of P taps: no bound test
+  for (; k0 + P <= K; k0 += P) {
+#pragma unroll
+    for (int j = 0; j < P; ++j) win[P + j] = at(k0 + P + j);
+#pragma unroll
+    for (int j = 0; j < P; ++j) {
+      const W w = taps[k0 + j];
+      if (!SKIPZ || w != W(0)) {
+#pragma unroll
+        for (int p = 0; p < P; ++p) acc[p] = fma(win[p + j], w, acc[p]);
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < P; ++j) win[j] = win[P + j];
+  }
+  if (k0 < K) {
+    // the last K - k0 < P taps
 #pragma unroll
     for (int j = 0; j < P; ++j) win[P + j] = at(k0 + P + j);
 #pragma unroll
@@ -69,9 +86,14 @@ __device__ __forceinline__ void tap_loop(W (&acc)[P], const W* taps, int K, At a
         for (int p = 0; p < P; ++p) acc[p] = fma(win[p + j], w, acc[p]);
       }
     }
-#pragma unroll
-    for (int j = 0; j < P; ++j) win[j] = win[P + j];
   }
+}
+
+// Value of line coordinate c (boundary mode applied) of a float32 input.
+__device__ __forceinline__ float staged_f32(const float* line, long long stride, long long c,
+                                            long long L, int mode, float cv) {
+  const long long m = (c >= 0 && c < L) ? c : map_coord(c, L, mode);
+  return m < 0 ? cv : __ldg(line + m * stride);
 }
 
 // Filter along the contiguous last axis (inner == 1). Block = (seg_threads,
@@ -96,9 +118,44 @@ __global__ void __launch_bounds__(256) k_rows(GArgs a, TapBlock<W> tb) {
   const W cv = fill_value<W>(a.cval, a.cval_as_input, a.tin);
   const long long rbase = row * a.L;
   if (row < a.outer) {
-    for (int j = threadIdx.x; j < span; j += blockDim.x) {
-      const long long m = map_coord(x0 - a.anchor + j, a.L, a.mode);
-      rb[j + (j >> 3)] = m < 0 ? cv : load_as<W>(a.in, rbase + m, a.tin);
+    const bool interior = x0 - a.anchor >= 0 && x0 - a.anchor + span <= a.L;
+    if (sizeof(W) == 4 && a.tin == DT_F32 && interior) {
+      // float32 input, span inside the row: plain loads, eight in flight
+      const float* line = static_cast<const float*>(a.in) + rbase + (x0 - a.anchor);
+      for (int jb = threadIdx.x; jb < span; jb += 8 * blockDim.x) {
+        float v[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const int j = jb + q * blockDim.x;
+          v[q] = j < span ? __ldg(line + j) : 0.f;
+        }
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const int j = jb + q * blockDim.x;
+          if (j < span) rb[j + (j >> 3)] = v[q];
+        }
+      }
+    } else if (sizeof(W) == 4 && a.tin == DT_F32) {
+      // float32 input: eight loads in flight per thread before the stores
+      const float* line = static_cast<const float*>(a.in) + rbase;
+      for (int jb = threadIdx.x; jb < span; jb += 8 * blockDim.x) {
+        float v[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const int j = jb + q * blockDim.x;
+          v[q] = j < span ? staged_f32(line, 1, x0 - a.anchor + j, a.L, a.mode, (float)cv) : 0.f;
+        }
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const int j = jb + q * blockDim.x;
+          if (j < span) rb[j + (j >> 3)] = v[q];
+        }
+      }
+    } else {
+      for (int j = threadIdx.x; j < span; j += blockDim.x) {
+        const long long m = map_coord(x0 - a.anchor + j, a.L, a.mode);
+        rb[j + (j >> 3)] = m < 0 ? cv : load_as<W>(a.in, rbase + m, a.tin);
+      }
     }
   }
   __syncthreads();
@@ -138,13 +195,51 @@ __global__ void __launch_bounds__(256) k_cols(GArgs a, TapBlock<W> tb) {
   const long long l0 = lt * kColTL;
   const W cv = fill_value<W>(a.cval, a.cval_as_input, a.tin);
   const long long obase = o * a.L;
-  for (int j = threadIdx.y; j < span; j += kColTY) {
-    W v = W(0);
-    if (i < a.inner) {
-      const long long m = map_coord(l0 - a.anchor + j, a.L, a.mode);
-      v = m < 0 ? cv : load_as<W>(a.in, (obase + m) * a.inner + i, a.tin);
+  const bool interior = l0 - a.anchor >= 0 && l0 - a.anchor + span <= a.L;
+  if (sizeof(W) == 4 && a.tin == DT_F32 && interior) {
+    // float32 input, span inside the line: a pointer walk, eight loads in flight
+    const long long stride = a.inner;
+    const float* col = static_cast<const float*>(a.in) + (obase + l0 - a.anchor) * stride + i;
+    for (int jb = threadIdx.y; jb < span; jb += 8 * kColTY) {
+      float v[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const int j = jb + q * kColTY;
+        v[q] = (j < span && i < a.inner) ? __ldg(col + (long long)j * stride) : 0.f;
+      }
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const int j = jb + q * kColTY;
+        if (j < span) buf[j * kColTI + threadIdx.x] = v[q];
+      }
     }
-    buf[j * kColTI + threadIdx.x] = v;
+  } else if (sizeof(W) == 4 && a.tin == DT_F32) {
+    // float32 input: eight loads in flight per thread before the stores
+    const float* col = static_cast<const float*>(a.in) + obase * a.inner + i;
+    for (int jb = threadIdx.y; jb < span; jb += 8 * kColTY) {
+      float v[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const int j = jb + q * kColTY;
+        v[q] = (j < span && i < a.inner)
+                   ? staged_f32(col, a.inner, l0 - a.anchor + j, a.L, a.mode, (float)cv)
+                   : 0.f;
+      }
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const int j = jb + q * kColTY;
+        if (j < span) buf[j * kColTI + threadIdx.x] = v[q];
+      }
+    }
+  } else {
+    for (int j = threadIdx.y; j < span; j += kColTY) {
+      W v = W(0);
+      if (i < a.inner) {
+        const long long m = map_coord(l0 - a.anchor + j, a.L, a.mode);
+        v = m < 0 ? cv : load_as<W>(a.in, (obase + m) * a.inner + i, a.tin);
+      }
+      buf[j * kColTI + threadIdx.x] = v;
+    }
   }
   __syncthreads();
   if (i >= a.inner) return;
