@@ -554,22 +554,8 @@ __global__ void __launch_bounds__(kThreads, 1)
         const uint32_t tbase = tmem + ((uint32_t)(32 * warp) << 16) + slot * (uint32_t)a.NB;
         const long long l = lb + 32 * warp + lane;  // this thread's output
         const int nq = a.NL / 32;
-        // per column group: read and sum the accumulators, release the slot
-        // after the last group's reads, then store
-        for (int q = 0; q < nq; ++q) {
-          const uint32_t col = tbase + 32 * q;
-          float v[32], x[32];
-          tmem_ld32(col, v);
-          for (int h = 1; h <= a.NHH; ++h) {
-            tmem_ld32(col + h * a.NL, x);
-#pragma unroll
-            for (int e = 0; e < 32; ++e) v[e] = __fadd_rn(v[e], x[e]);
-          }
-          if (q == nq - 1) {
-            tmem_fence_before();
-            mbar_arrive(&acce[slot]);
-          }
-          if (l >= a.L) continue;
+        auto store_group = [&](int q, const float (&v)[32]) {
+          if (l >= a.L) return;
           const long long n = r.n0 + 32 * q;  // first line of this column group
           if (CONTIG) {
             // lines are rows: a warp stores 32 consecutive outputs of a row
@@ -588,6 +574,38 @@ __global__ void __launch_bounds__(kThreads, 1)
               for (int e = 0; e < 32; ++e)
                 if (n + e < a.inner) dst[e] = v[e];
             }
+          }
+        };
+        auto sum_group = [&](int q, float (&v)[32]) {
+          const uint32_t col = tbase + 32 * q;
+          float x[32];
+          tmem_ld32(col, v);
+          for (int h = 1; h <= a.NHH; ++h) {
+            tmem_ld32(col + h * a.NL, x);
+#pragma unroll
+            for (int e = 0; e < 32; ++e) v[e] = __fadd_rn(v[e], x[e]);
+          }
+        };
+        if (nq <= 2) {
+          // read every column group, release the slot, then store: the MMA
+          // threads wait for this slot when the ring has no spare one
+          float v0[32], v1[32];
+          sum_group(0, v0);
+          if (nq == 2) sum_group(1, v1);
+          tmem_fence_before();
+          mbar_arrive(&acce[slot]);
+          store_group(0, v0);
+          if (nq == 2) store_group(1, v1);
+        } else {
+          // per column group; the slot is released after the last group's reads
+          for (int q = 0; q < nq; ++q) {
+            float v[32];
+            sum_group(q, v);
+            if (q == nq - 1) {
+              tmem_fence_before();
+              mbar_arrive(&acce[slot]);
+            }
+            store_group(q, v);
           }
         }
       }
