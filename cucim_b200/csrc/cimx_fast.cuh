@@ -685,6 +685,17 @@ int launch_slab_kb(SlabArgs& a, cudaStream_t st) {
 // x fill value in constant mode: that is how cuCIM's second pass sees the
 // first pass's output beyond the row ends. The arithmetic, tap order and
 // rounding are those of k_slab.
+// Exact float value of an unsigned integer below 2^23 without the conversion
+// unit: the integer placed in the mantissa of 2^23, minus 2^23.
+template <class T>
+__device__ __forceinline__ float exact_float(T v) {
+  if constexpr (sizeof(T) == 4) {
+    return static_cast<float>(v);
+  } else {
+    return __fsub_rn(__uint_as_float(0x4B000000u | static_cast<uint32_t>(v)), 8388608.0f);
+  }
+}
+
 template <int K>
 struct RowArgs {
   const void* in;
@@ -816,10 +827,10 @@ __global__ void __launch_bounds__(row_max_threads<K>()) k_rowstream(const RowArg
           } else {
             const typename Vec4<T>::type q =
                 *reinterpret_cast<const typename Vec4<T>::type*>(pre + (size_t)u * NT * 4);
-            v[0] = static_cast<float>(q.x);
-            v[1] = static_cast<float>(q.y);
-            v[2] = static_cast<float>(q.z);
-            v[3] = static_cast<float>(q.w);
+            v[0] = exact_float(q.x);
+            v[1] = exact_float(q.y);
+            v[2] = exact_float(q.z);
+            v[3] = exact_float(q.w);
           }
           // y chain, rounded through D into this step's row buffer
           float acc[4] = {0.f, 0.f, 0.f, 0.f};
@@ -831,7 +842,7 @@ __global__ void __launch_bounds__(row_max_threads<K>()) k_rowstream(const RowArg
           float* R = R0 + (s & 1) * RS;
           float iv[4];
 #pragma unroll
-          for (int e = 0; e < 4; ++e) iv[e] = static_cast<float>(out_cast<D>(acc[e]));
+          for (int e = 0; e < 4; ++e) iv[e] = exact_float(out_cast<D>(acc[e]));
           *reinterpret_cast<float4*>(R + c0) = make_float4(iv[0], iv[1], iv[2], iv[3]);
           for (uint32_t bits = own; bits; bits &= bits - 1) {
             const int i = __ffs(bits) - 1;
