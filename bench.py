@@ -168,7 +168,10 @@ def step_ops(ndi, x, outs):
     ndi.uniform_filter(x, 5, output=u)
 
 
-LAUNCHES_PER_STEP = 10  # each op: one streamed pass (axis 0) + one fused (y, x) slab launch
+LAUNCHES_PER_STEP = 10  # each op: one streamed pass (axis 0) + one fused (y, x) launch
+
+# DRAM bytes per launch measured by ncu on a 64 x 1024 x 1024 stack
+SLAB_TRAFFIC_64 = {"slab f32->f32 gaussian y,x K=17,17": 268.507136e6 + 227.813888e6}
 
 
 def reduce_step_time(ms, world, device, dist, torch):
@@ -590,6 +593,13 @@ def main():
         roof = {"bound": "hbm", "kernel": name, "achieved": kr["gbs"], "peak": hbm,
                 "unit": "GB/s", "frac": kr["gbs"] / hbm, "traffic": None,
                 "peak_source": "measured" if peaks else "fallback"}
+        if name in SLAB_TRAFFIC_64 and args.shape is None:
+            # DRAM bytes of the same kernel captured by ncu on a 64-slice stack,
+            # scaled to the 512-slice launch (traffic grows with the slices)
+            roof["traffic"] = SLAB_TRAFFIC_64[name] * SHAPE[0] / 64
+            roof["traffic_source"] = ("ncu dram__bytes_read + dram__bytes_write of the same kernel on "
+                                      "64 x 1024 x 1024, x 512/64 (profiles/"
+                                      "k_slab_f32_gaussian_yx_64x1024x1024.md)")
         cpu = None
         if not args.no_cpu:
             cpu = cpu_baseline(res["x"].numpy())
