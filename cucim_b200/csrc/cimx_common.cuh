@@ -38,10 +38,46 @@ __host__ __device__ inline int dtype_size(int dt) {
 
 // ---------------------------------------------------------------- casts
 
+// Float -> 8/16-bit integer conversion of the GPU: truncation toward zero,
+// saturation to the 16-bit range (unsigned for a uint16 target, signed for
+// the 8-bit and int16 targets), NaN -> 0; an 8-bit target keeps the low 8
+// bits. This is the conversion a scalar store of the C cast compiles to. It
+// is written out in PTX because an out-of-range C cast is undefined, and the
+// compiler may fold a narrow conversion whose result is widened again (packed
+// into a vector, merged with another store, converted back to float) into
+// one wider conversion, which wraps instead of saturating.
+template <class B, class A>
+__device__ __forceinline__ uint32_t cvt_rzi16(A a) {
+  unsigned short u;
+  if constexpr (std::is_same<A, double>::value) {
+    if constexpr (std::is_same<B, unsigned short>::value)
+      asm("cvt.rzi.u16.f64 %0, %1;" : "=h"(u) : "d"(a));
+    else
+      asm("cvt.rzi.s16.f64 %0, %1;" : "=h"(u) : "d"(a));
+  } else {
+    const float f = static_cast<float>(a);
+    if constexpr (std::is_same<B, unsigned short>::value)
+      asm("cvt.rzi.u16.f32 %0, %1;" : "=h"(u) : "f"(f));
+    else
+      asm("cvt.rzi.s16.f32 %0, %1;" : "=h"(u) : "f"(f));
+  }
+  return u;
+}
+
 template <class B, class A>
 __device__ __forceinline__ B out_cast(A a) {
   if constexpr (std::is_same<B, __half>::value) {
     return __float2half_rn(static_cast<float>(a));
+  } else if constexpr (std::is_floating_point<A>::value && std::is_integral<B>::value &&
+                       sizeof(B) <= 2) {
+    if constexpr (!std::is_signed<B>::value) {
+      // (a >= 0) ? (B)a : -(B)(-a); NaN takes the second side and gives 0
+      const bool neg = !(a >= 0);
+      const uint32_t v = cvt_rzi16<B>(neg ? -a : a);
+      return static_cast<B>(neg ? 0u - v : v);
+    } else {
+      return static_cast<B>(cvt_rzi16<B>(a));
+    }
   } else if constexpr (std::is_floating_point<A>::value && !std::is_signed<B>::value) {
     return (a >= 0) ? static_cast<B>(a) : static_cast<B>(-static_cast<B>(-a));
   } else {
@@ -106,10 +142,11 @@ __device__ __forceinline__ W fill_value(double cval, int as_input, int dt) {
   switch (dt) {
     case DT_F32: return static_cast<W>(static_cast<float>(cval));
     case DT_F64: return static_cast<W>(cval);
-    case DT_U8: return static_cast<W>(static_cast<unsigned char>(cval));
-    case DT_I8: return static_cast<W>(static_cast<signed char>(cval));
-    case DT_U16: return static_cast<W>(static_cast<unsigned short>(cval));
-    case DT_I16: return static_cast<W>(static_cast<short>(cval));
+    // 8/16-bit: the GPU conversion of the C cast, written out (cvt_rzi16)
+    case DT_U8: return static_cast<W>(static_cast<unsigned char>(cvt_rzi16<unsigned char>(cval)));
+    case DT_I8: return static_cast<W>(static_cast<signed char>(cvt_rzi16<signed char>(cval)));
+    case DT_U16: return static_cast<W>(static_cast<unsigned short>(cvt_rzi16<unsigned short>(cval)));
+    case DT_I16: return static_cast<W>(static_cast<short>(cvt_rzi16<short>(cval)));
     case DT_U32: return static_cast<W>(static_cast<unsigned int>(cval));
     case DT_I32: return static_cast<W>(static_cast<int>(cval));
     case DT_U64: case DT_U64Q: return static_cast<W>(static_cast<unsigned long long>(cval));

@@ -40,6 +40,32 @@ template <> struct Vec4<float> { using type = float4; };
 template <> struct Vec4<uint16_t> { using type = ushort4; };
 template <> struct Vec4<uint8_t> { using type = uchar4; };
 
+// Exact float value of an unsigned integer below 2^23 without the conversion
+// unit: the integer placed in the mantissa of 2^23, minus 2^23.
+template <class T>
+__device__ __forceinline__ float exact_float(T v) {
+  if constexpr (sizeof(T) == 4) {
+    return static_cast<float>(v);
+  } else {
+    return __fsub_rn(__uint_as_float(0x4B000000u | static_cast<uint32_t>(v)), 8388608.0f);
+  }
+}
+
+// cast<D>(a) of an intermediate that stays on chip, as the float the next
+// pass reads (out_cast writes the narrowing conversion out explicitly, so
+// widening its result again keeps the narrow value)
+template <class D>
+__device__ __forceinline__ float narrow_float(float a) {
+  if constexpr (sizeof(D) == 4) return a;
+  else return exact_float(out_cast<D>(a));
+}
+
+// cast<D>(a) as stored
+template <class D>
+__device__ __forceinline__ D narrow_cast(float a) {
+  return out_cast<D>(a);
+}
+
 template <class T>
 __device__ __forceinline__ void load4(const T* p, float (&v)[4]) {
   const typename Vec4<T>::type q = *reinterpret_cast<const typename Vec4<T>::type*>(p);
@@ -52,10 +78,10 @@ __device__ __forceinline__ void load4(const T* p, float (&v)[4]) {
 template <class D>
 __device__ __forceinline__ void store4(D* p, float a, float b, float c, float d) {
   typename Vec4<D>::type q;
-  q.x = out_cast<D>(a);
-  q.y = out_cast<D>(b);
-  q.z = out_cast<D>(c);
-  q.w = out_cast<D>(d);
+  q.x = narrow_cast<D>(a);
+  q.y = narrow_cast<D>(b);
+  q.z = narrow_cast<D>(c);
+  q.w = narrow_cast<D>(d);
   *reinterpret_cast<typename Vec4<D>::type*>(p) = q;
 }
 
@@ -103,6 +129,7 @@ __device__ __forceinline__ void cp_async_vec4(T* dst, const T* src) {
   else if constexpr (sizeof(T) == 2) cp_async8(dst, src);
   else cp_async4(dst, src);
 }
+
 
 // ---------------------------------------------------------------- (a)
 
@@ -567,10 +594,10 @@ __global__ void __launch_bounds__(256, kSlabMinBlocks) k_slab(const __grid_const
         f2* d1 = s_mid + (rg / 2) * G::RXQ + pad8(e + 1);
 #pragma unroll
         for (int p = 0; p < P; p += 2) {
-          const float a0 = f0 ? cx : static_cast<float>(out_cast<D>(lo2(acc[p])));
-          const float b0 = f0 ? cx : static_cast<float>(out_cast<D>(lo2(acc[p + 1])));
-          const float a1 = f1 ? cx : static_cast<float>(out_cast<D>(hi2(acc[p])));
-          const float b1 = f1 ? cx : static_cast<float>(out_cast<D>(hi2(acc[p + 1])));
+          const float a0 = f0 ? cx : narrow_float<D>(lo2(acc[p]));
+          const float b0 = f0 ? cx : narrow_float<D>(lo2(acc[p + 1]));
+          const float a1 = f1 ? cx : narrow_float<D>(hi2(acc[p]));
+          const float b1 = f1 ? cx : narrow_float<D>(hi2(acc[p + 1]));
           d0[(p / 2) * G::RXQ] = pack2(a0, b0);
           d1[(p / 2) * G::RXQ] = pack2(a1, b1);
         }
@@ -582,9 +609,9 @@ __global__ void __launch_bounds__(256, kSlabMinBlocks) k_slab(const __grid_const
           const long long yy = y0 + rg + p;
           if (yy >= a.Y) continue;
           if (c0 >= 0 && c0 < kSlabTX && x0 + c0 < a.X)
-            out[yy * a.X + x0 + c0] = out_cast<D>(lo2(acc[p]));
+            out[yy * a.X + x0 + c0] = narrow_cast<D>(lo2(acc[p]));
           if (c0 + 1 >= 0 && c0 + 1 < kSlabTX && x0 + c0 + 1 < a.X)
-            out[yy * a.X + x0 + c0 + 1] = out_cast<D>(hi2(acc[p]));
+            out[yy * a.X + x0 + c0 + 1] = narrow_cast<D>(hi2(acc[p]));
         }
       }
     }
@@ -623,7 +650,7 @@ __global__ void __launch_bounds__(256, kSlabMinBlocks) k_slab(const __grid_const
         } else {
 #pragma unroll
           for (int p = 0; p < P; ++p)
-            if (p < left) orow[p] = out_cast<D>(v[p]);
+            if (p < left) orow[p] = narrow_cast<D>(v[p]);
         }
       }
     }
@@ -685,16 +712,6 @@ int launch_slab_kb(SlabArgs& a, cudaStream_t st) {
 // x fill value in constant mode: that is how cuCIM's second pass sees the
 // first pass's output beyond the row ends. The arithmetic, tap order and
 // rounding are those of k_slab.
-// Exact float value of an unsigned integer below 2^23 without the conversion
-// unit: the integer placed in the mantissa of 2^23, minus 2^23.
-template <class T>
-__device__ __forceinline__ float exact_float(T v) {
-  if constexpr (sizeof(T) == 4) {
-    return static_cast<float>(v);
-  } else {
-    return __fsub_rn(__uint_as_float(0x4B000000u | static_cast<uint32_t>(v)), 8388608.0f);
-  }
-}
 
 template <int K>
 struct RowArgs {
@@ -842,7 +859,7 @@ __global__ void __launch_bounds__(row_max_threads<K>()) k_rowstream(const RowArg
           float* R = R0 + (s & 1) * RS;
           float iv[4];
 #pragma unroll
-          for (int e = 0; e < 4; ++e) iv[e] = exact_float(out_cast<D>(acc[e]));
+          for (int e = 0; e < 4; ++e) iv[e] = narrow_float<D>(acc[e]);
           *reinterpret_cast<float4*>(R + c0) = make_float4(iv[0], iv[1], iv[2], iv[3]);
           for (uint32_t bits = own; bits; bits &= bits - 1) {
             const int i = __ffs(bits) - 1;

@@ -1,6 +1,7 @@
 // cimx_fast_u16.cu — instantiations of the fast kernels (cimx_fast.cuh) for
 // uint16_t input. Split by input dtype so the kernels compile in parallel.
 #include "cimx_fast.cuh"
+#include "cimx_vol.cuh"
 
 namespace cimx {
 
@@ -19,6 +20,12 @@ int launch_slab_u16(SlabArgs& a, int tout, cudaStream_t st) {
   using namespace fast;
   if (tout == DT_F32) return launch_slab_td<uint16_t, float>(a, st);
   if (tout == DT_U16) return launch_slab_td<uint16_t, uint16_t>(a, st);
+  return CIMX_FUSED_DECLINED;
+}
+
+int launch_vol_u16(const VolArgs& v, int tout, cudaStream_t st) {
+  if (tout == DT_F32) return vol::launch_vol_td<uint16_t, float>(v, st);
+  if (tout == DT_U16) return vol::launch_vol_td<uint16_t, uint16_t>(v, st);
   return CIMX_FUSED_DECLINED;
 }
 

@@ -1,6 +1,7 @@
 // cimx_fast_u8.cu — instantiations of the fast kernels (cimx_fast.cuh) for
 // uint8_t input. Split by input dtype so the kernels compile in parallel.
 #include "cimx_fast.cuh"
+#include "cimx_vol.cuh"
 
 namespace cimx {
 
@@ -22,6 +23,13 @@ int launch_slab_u8(SlabArgs& a, int tout, cudaStream_t st) {
   if (tout == DT_F32) return launch_slab_td<uint8_t, float>(a, st);
   if (tout == DT_U8) return launch_slab_td<uint8_t, uint8_t>(a, st);
   if (tout == DT_U16) return launch_slab_td<uint8_t, uint16_t>(a, st);
+  return CIMX_FUSED_DECLINED;
+}
+
+int launch_vol_u8(const VolArgs& v, int tout, cudaStream_t st) {
+  if (tout == DT_F32) return vol::launch_vol_td<uint8_t, float>(v, st);
+  if (tout == DT_U8) return vol::launch_vol_td<uint8_t, uint8_t>(v, st);
+  if (tout == DT_U16) return vol::launch_vol_td<uint8_t, uint16_t>(v, st);
   return CIMX_FUSED_DECLINED;
 }
 

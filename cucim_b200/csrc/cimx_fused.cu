@@ -1,7 +1,9 @@
 // cimx_fused.cu — decides whether a pass list runs on the fast kernels
-// (cimx_fast.cuh) and schedules them: passes along leading axes are streamed
-// one launch each (k_stream), the passes along the last two axes run fused in
-// one slab launch (k_slab). Intermediates follow cuCIM's _run_1d_filters
+// (cimx_fast.cuh, cimx_vol.cuh) and schedules them: a 3-D filter with short
+// taps on all three axes is one launch of the volume kernel (k_vol);
+// otherwise passes along leading axes are streamed one launch each
+// (k_stream), the passes along the last two axes run fused in one slab
+// launch (k_slab or k_rowstream). Intermediates follow cuCIM's _run_1d_filters
 // ping-pong: every pass writes the output dtype, the last launch writes the
 // caller's output, one scratch buffer takes the others.
 #include <algorithm>
@@ -90,6 +92,49 @@ void fill_slab_pass(SlabPass& s, const PassDesc& d, const Trimmed& t, int pass_i
   std::copy(t.w, t.w + t.K, s.w);
 }
 
+int launch_vol(const VolArgs& v, int tin, int tout, cudaStream_t st) {
+  switch (tin) {
+    case DT_F32: return launch_vol_f32(v, tout, st);
+    case DT_U16: return launch_vol_u16(v, tout, st);
+    case DT_U8: return launch_vol_u8(v, tout, st);
+    default: return CIMX_FUSED_DECLINED;
+  }
+}
+
+// z, y and x passes over the last three axes with the same short taps: one
+// launch of the volume kernel, no intermediate volume
+int try_vol(const CimxArray* in, const CimxArray* out, const PassDesc* ds, cudaStream_t st) {
+  const int nd = in->ndim;
+  const int D = out->dtype;
+  if (!fast_pair(in->dtype, D)) return CIMX_FUSED_DECLINED;
+  Trimmed t[3];
+  for (int i = 0; i < 3; ++i)
+    if (!trim(ds[i], 5, t[i])) return CIMX_FUSED_DECLINED;
+  const int K = t[0].K;
+  if ((K != 3 && K != 5) || t[1].K != K || t[2].K != K) return CIMX_FUSED_DECLINED;
+  // the x chain takes its halo from the neighbouring lanes: centred taps,
+  // and no wrap-around (whose halo lies at the far end of the row)
+  if (t[2].anchor != K / 2 || ds[2].mode == CIMX_MODE_GRID_WRAP) return CIMX_FUSED_DECLINED;
+  const long long X = in->shape[nd - 1], Y = in->shape[nd - 2], Z = in->shape[nd - 3];
+  long long B = 1;
+  for (int k = 0; k < nd - 3; ++k) B *= in->shape[k];
+  if (X % 4 != 0 || X < 8 || Y < 1 || Z < 1 || B < 1) return CIMX_FUSED_DECLINED;
+  if (Y * X >= (1LL << 31) || Z >= (1LL << 31)) return CIMX_FUSED_DECLINED;
+  if (!aligned(in->data, 4 * dtype_size(in->dtype)) || !aligned(out->data, 4 * dtype_size(D)))
+    return CIMX_FUSED_DECLINED;
+  VolArgs v{};
+  v.in = in->data;
+  v.out = out->data;
+  v.B = B;
+  v.Z = Z;
+  v.Y = Y;
+  v.X = X;
+  fill_slab_pass(v.pz, ds[0], t[0], in->dtype);
+  fill_slab_pass(v.py, ds[1], t[1], D);
+  fill_slab_pass(v.px, ds[2], t[2], D);
+  return launch_vol(v, in->dtype, D, st);
+}
+
 }  // namespace
 
 int try_fused(const CimxArray* in, const CimxArray* out, PassDesc* ds, int npasses,
@@ -102,6 +147,12 @@ int try_fused(const CimxArray* in, const CimxArray* out, PassDesc* ds, int npass
   for (int i = 0; i < npasses; ++i) {
     if (ds[i].axis <= prev_axis || ds[i].w64) return CIMX_FUSED_DECLINED;
     prev_axis = ds[i].axis;
+  }
+
+  if (nd >= 3 && npasses == 3 && ds[0].axis == nd - 3 && ds[1].axis == nd - 2 &&
+      ds[2].axis == nd - 1) {
+    const int rc = try_vol(in, out, ds, st);
+    if (rc != CIMX_FUSED_DECLINED) return rc;
   }
 
   // leading axes are streamed, the last two axes go to the slab kernel

@@ -32,6 +32,15 @@ struct SlabArgs {
   SlabPass py, px;
 };
 
+// The three passes of a 3-D filter (z, y, x over the last three axes), for
+// the single-launch volume kernel (cimx_vol.cuh).
+struct VolArgs {
+  const void* in;
+  void* out;
+  long long B, Z, Y, X;
+  SlabPass pz, py, px;
+};
+
 // Runs the whole pass list `ds` (already resolved against the input shape)
 // in fast launches when they cover it. Returns CIMX_OK, a negative error, or
 // CIMX_FUSED_DECLINED (nothing was launched).
@@ -49,6 +58,11 @@ int launch_stream_u16(const PassDesc& d, const float* w, int K, int anchor, bool
                       const void* in, int tout, void* out, cudaStream_t st);
 int launch_stream_u8(const PassDesc& d, const float* w, int K, int anchor, bool interior_zero,
                      const void* in, int tout, void* out, cudaStream_t st);
+
+// single-launch 3-D filter, by input dtype; equal K in {3, 5} on every axis
+int launch_vol_f32(const VolArgs& v, int tout, cudaStream_t st);
+int launch_vol_u16(const VolArgs& v, int tout, cudaStream_t st);
+int launch_vol_u8(const VolArgs& v, int tout, cudaStream_t st);
 
 // fused (y, x) slab launch, by input dtype
 int launch_slab_f32(SlabArgs& a, int tout, cudaStream_t st);

@@ -8,6 +8,7 @@ CUDA tensors, CuPy arrays or any __cuda_array_interface__ / DLPack object;
 results come back as the input's array type.
 """
 
+import contextlib
 import ctypes
 import math
 import warnings
@@ -95,6 +96,25 @@ TENSOR_BF16X3 = "tensor_bf16x3"
 _TENSOR_FLAGS = {TENSOR: _lib.L_TENSOR_TF32X3, TENSOR_BF16X3: _lib.L_TENSOR_BF16X3}
 
 
+_EXTRA_LIB_FLAGS = 0
+
+
+@contextlib.contextmanager
+def pass_by_pass():
+    """Within this block every filter runs one launch per 1-D pass, through
+    one scratch volume of the output dtype (the schedule of _run_1d_filters,
+    _vendored/_ndimage_filters_core.py:124-163), instead of the fused
+    kernels. The results are bit-identical; it only runs slower. A testing
+    and debugging aid, not thread-safe."""
+    global _EXTRA_LIB_FLAGS
+    old = _EXTRA_LIB_FLAGS
+    _EXTRA_LIB_FLAGS = old | _lib.L_NO_FUSION
+    try:
+        yield
+    finally:
+        _EXTRA_LIB_FLAGS = old
+
+
 def _run(input, specs, output, cval, algorithm=None):
     """Apply the pass list to `input` into `output` (FLT:363-396 semantics)."""
     x = _arrays.as_tensor(input)
@@ -103,9 +123,9 @@ def _run(input, specs, output, cval, algorithm=None):
     xc = x.contiguous()
     slot = _arrays.output_slot(output, input, xc)
     out_dt = slot.dtype
-    lib_flags = 0
+    lib_flags = _EXTRA_LIB_FLAGS
     if algorithm in _TENSOR_FLAGS:
-        lib_flags, algorithm = _TENSOR_FLAGS[algorithm], None
+        lib_flags, algorithm = lib_flags | _TENSOR_FLAGS[algorithm], None
     pl = _build_passes(_arrays.np_dtype(xc), out_dt, xc.dim(), specs, cval, algorithm)
     arr = pl.array()
     a_in = _arrays.to_cimx(xc)

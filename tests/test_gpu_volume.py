@@ -1,0 +1,176 @@
+"""The single-launch 3-D kernel: a filter with 3 or 5 taps on each of the
+last three axes runs its z, y and x passes in one launch. Its outputs must be
+bit-identical to the oracle and to the pass-by-pass schedule (one launch per
+pass through a scratch volume). The shapes have rows of a multiple of 4
+elements (the kernel's condition) and cover partial tiles in y and x, short
+and chunked z, a leading batch axis and rows of only 8 elements."""
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import restate as R
+
+pytestmark = pytest.mark.gpu
+
+MODES = ["reflect", "mirror", "nearest", "wrap", "constant"]
+SHAPES = [(9, 70, 128), (7, 33, 244), (3, 9, 8), (2, 3, 19, 36), (130, 20, 16), (1, 66, 40)]
+
+
+def dev(a):
+    return torch.as_tensor(np.ascontiguousarray(a)).cuda()
+
+
+def host(t):
+    return t.cpu().numpy()
+
+
+@pytest.fixture(scope="module")
+def ndi(cuda):
+    from cucim_b200 import ndimage
+
+    return ndimage
+
+
+def _ints(shape, dtype, seed, hi=250):
+    return np.random.default_rng(seed).integers(0, hi, shape).astype(dtype)
+
+
+@pytest.mark.parametrize("shape", SHAPES)
+@pytest.mark.parametrize("func", ["sobel", "prewitt"])
+@pytest.mark.parametrize("tin,tout", [(np.uint16, np.float32), (np.uint8, np.uint8),
+                                      (np.float32, np.float32), (np.uint8, np.float32),
+                                      (np.uint8, np.uint16)])
+def test_volume_sobel_prewitt(ndi, shape, func, tin, tout):
+    x = _ints(shape, tin, 3)
+    xd = dev(x)
+    for axis in (-3, -2, -1):
+        got = host(getattr(ndi, func)(xd, axis, output=tout))
+        exp = getattr(R, func)(x, axis, output=tout)
+        np.testing.assert_array_equal(got, exp)
+
+
+@pytest.mark.parametrize("mode", MODES)
+@pytest.mark.parametrize("size", [3, 5])
+@pytest.mark.parametrize("shape", [(9, 70, 128), (7, 33, 244), (2, 3, 19, 36)])
+def test_volume_uniform_u16_exact(ndi, mode, size, shape):
+    x = _ints(shape, np.uint16, 1, hi=65536)
+    got = host(ndi.uniform_filter(dev(x), size, output=np.uint16, mode=mode, cval=7))
+    exp = R.uniform_filter(x, size, output=np.uint16, mode=mode, cval=7)
+    np.testing.assert_array_equal(got, exp)
+
+
+@pytest.mark.parametrize("mode", MODES)
+@pytest.mark.parametrize("shape", [(9, 70, 128), (130, 20, 16), (3, 9, 8)])
+def test_volume_float_modes(ndi, mode, shape):
+    x = np.random.default_rng(5).standard_normal(shape).astype(np.float32)
+    xd = dev(x)
+    for got, exp in [
+        (ndi.gaussian_filter(xd, 0.5, mode=mode, cval=-0.5),
+         R.gaussian_filter(x, 0.5, mode=mode, cval=-0.5)),
+        (ndi.uniform_filter(xd, 3, mode=mode, cval=1.25),
+         R.uniform_filter(x, 3, mode=mode, cval=1.25)),
+        (ndi.sobel(xd, 1, mode=mode, cval=2.0), R.sobel(x, 1, mode=mode, cval=2.0)),
+    ]:
+        np.testing.assert_array_equal(host(got), exp)
+
+
+def test_volume_mixed_modes_and_origins(ndi):
+    x = np.random.default_rng(6).standard_normal((11, 45, 132)).astype(np.float32)
+    xd = dev(x)
+    for mode, origin in [(("constant", "mirror", "nearest"), 0),
+                         (("reflect", "constant", "constant"), 0),
+                         (("mirror", "nearest", "constant"), (1, -1, 0)),
+                         (("wrap", "wrap", "reflect"), 0),
+                         ("nearest", (0, 0, 1))]:
+        got = host(ndi.uniform_filter(xd, 3, mode=mode, cval=0.75, origin=origin))
+        exp = R.uniform_filter(x, 3, mode=mode, cval=0.75, origin=origin)
+        np.testing.assert_array_equal(got, exp)
+
+
+def test_volume_batch_axis(ndi):
+    # passes over the last three axes of a 4-D array: the batch loop
+    x = _ints((3, 5, 21, 40), np.uint16, 8, hi=65536)
+    got = host(ndi.uniform_filter(dev(x), 5, output=np.uint16, axes=(1, 2, 3), mode="mirror"))
+    exp = R.uniform_filter(x, 5, output=np.uint16, axes=(1, 2, 3), mode="mirror")
+    np.testing.assert_array_equal(got, exp)
+
+
+def test_volume_nonfinite_and_zero_taps(ndi):
+    # the derivative's zero tap is skipped: inf and nan do not leak through it
+    x = np.random.default_rng(7).standard_normal((6, 20, 64)).astype(np.float32)
+    x[2, 5, 10] = np.inf
+    x[4, 11, 40] = np.nan
+    xd = dev(x)
+    for axis in range(3):
+        np.testing.assert_array_equal(host(ndi.sobel(xd, axis)), R.sobel(x, axis))
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.uint16])
+def test_volume_matches_pass_by_pass(ndi, dtype):
+    """At a larger size: the single launch against one launch per pass."""
+    shape = (40, 300, 1000)
+    if dtype == np.uint16:
+        x = _ints(shape, dtype, 9, hi=65536)
+        out = np.float32
+    else:
+        x = np.random.default_rng(9).random(shape, dtype=np.float32)
+        out = np.float32
+    xd = dev(x)
+    calls = [lambda: ndi.sobel(xd, 0, output=out), lambda: ndi.sobel(xd, 2, output=out),
+             lambda: ndi.uniform_filter(xd, 5, output=dtype),
+             lambda: ndi.prewitt(xd, 1, output=out, mode="constant", cval=3.0)]
+    for call in calls:
+        got = call()
+        with ndi.pass_by_pass():
+            exp = call()
+        assert torch.equal(got, exp)
+
+
+@pytest.mark.parametrize("shape", [(64, 128), (40, 96), (7, 50, 72), (300, 260)])
+@pytest.mark.parametrize("tout", [np.uint16, np.uint8])
+def test_narrowed_intermediates_2d(ndi, shape, tout):
+    """Sobel of uint8 into uint8 / uint16: the first pass's negative and
+    out-of-range values are narrowed as cast<D>() stores them (wrap for
+    negatives, saturation above the range) before the next pass reads them,
+    also where the intermediate never leaves the chip (row-streaming and
+    slab kernels)."""
+    x = _ints(shape, np.uint8, 11, hi=256)
+    xd = dev(x)
+    for axis in range(len(shape)):
+        got = host(ndi.sobel(xd, axis, output=tout))
+        np.testing.assert_array_equal(got, R.sobel(x, axis, output=tout))
+    got = host(ndi.uniform_filter(xd, 5, output=tout))
+    np.testing.assert_array_equal(got, R.uniform_filter(x, 5, output=tout))
+
+
+@pytest.mark.parametrize("tout", [np.uint16, np.uint8])
+def test_narrowed_outputs_pass_by_pass(ndi, tout):
+    """The one-launch-per-pass kernels narrow out-of-range results the same
+    way (saturation for uint16, int16 saturation then the low 8 bits for
+    uint8)."""
+    x = _ints((9, 70, 128), np.uint8, 12, hi=256)
+    xd = dev(x)
+    with ndi.pass_by_pass():
+        for axis in range(3):
+            got = host(ndi.sobel(xd, axis, output=tout))
+            np.testing.assert_array_equal(got, R.sobel(x, axis, output=tout))
+
+
+@pytest.mark.parametrize("dtype,cval", [(np.uint8, 300.0), (np.uint8, -5.0), (np.uint16, 70000.0),
+                                        (np.uint16, -3.0), (np.int16, 40000.0)])
+@pytest.mark.parametrize("shape", [(40, 96), (6, 20, 64)])
+def test_out_of_range_fill_values(ndi, dtype, cval, shape):
+    # constant mode with a fill value outside the dtype's range: the
+    # shared-memory kernel's rule converts it to the input dtype first
+    x = _ints(shape, dtype, 13, hi=200)
+    got = host(ndi.uniform_filter(dev(x), 3, mode="constant", cval=cval))
+    np.testing.assert_array_equal(got, R.uniform_filter(x, 3, mode="constant", cval=cval))
+
+
+def test_volume_status_clean(ndi):
+    from cucim_b200 import _lib
+
+    ndi.sobel(dev(np.ones((8, 16, 32), np.float32)), 0)
+    torch.cuda.synchronize()
+    assert _lib.lib.cimx_device_status(1) == 0
