@@ -33,6 +33,7 @@
 #pragma once
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <mutex>
 
@@ -43,8 +44,13 @@
 namespace cimx {
 namespace vol {
 
-constexpr int kNW = 16;              // warps per CTA
-constexpr int kNT = 32 * kNW;
+// 16 warps per CTA, one CTA per SM; region rows per warp: 4 for 3 taps,
+// 3 for 5 taps (the ring of five slices needs the registers). Measured on a
+// 512 x 1024 x 1024 uint16 stack, 24 or 32 warps with fewer rows each ran
+// slower (register spills, more halo rows).
+constexpr int kNW = 16;
+constexpr int kM3 = 4;
+constexpr int kM5 = 3;
 constexpr int kRX = 128;             // region columns (4 per lane)
 constexpr int kHX = 4;               // halo columns on each side (one lane)
 constexpr int kTX = kRX - 2 * kHX;   // output columns per tile
@@ -65,21 +71,21 @@ struct VolKArgs {
   unsigned long long wz2[K], wy2[K];  // z and y taps, duplicated into both f32x2 lanes
 };
 
-// Region rows are one per (warp, group): M * kNW; a tile stores the
-// M * kNW - (K - 1) rows whose y windows lie inside the region.
-template <int K, int M> constexpr int vol_ry() { return M * kNW; }
-template <int K, int M> constexpr int vol_out_rows() { return M * kNW - (K - 1); }
+// NW warps per CTA. Region rows are one per (warp, group): M * NW; a tile
+// stores the M * NW - (K - 1) rows whose y windows lie inside the region.
+template <int K, int M, int NW> constexpr int vol_ry() { return M * NW; }
+template <int K, int M, int NW> constexpr int vol_out_rows() { return M * NW - (K - 1); }
 // plane rows allocated: the y chains of the last warp read K - 1 rows past
 // the region (never written; they only feed rows that are not stored)
-template <int K, int M> constexpr int vol_plane_rows() { return M * kNW + K - 1; }
+template <int K, int M, int NW> constexpr int vol_plane_rows() { return M * NW + K - 1; }
 template <class T> constexpr int vol_pf() { return sizeof(T) == 4 ? 3 : 5; }
-template <class T, int K, int M>
+template <class T, int K, int M, int NW>
 constexpr size_t vol_pre_bytes() {
-  return (size_t)(vol_pf<T>() + 1) * M * kNW * kRX * sizeof(T);
+  return (size_t)(vol_pf<T>() + 1) * M * NW * kRX * sizeof(T);
 }
-template <class T, int K, int M>
+template <class T, int K, int M, int NW>
 constexpr size_t vol_smem() {
-  return vol_pre_bytes<T, K, M>() + 2 * (size_t)vol_plane_rows<K, M>() * kRX * sizeof(float);
+  return vol_pre_bytes<T, K, M, NW>() + 2 * (size_t)vol_plane_rows<K, M, NW>() * kRX * sizeof(float);
 }
 
 using fast::f2;
@@ -100,21 +106,24 @@ __device__ __forceinline__ float pick4(const float (&v)[4], int e) {
   return e == 0 ? v[0] : e == 1 ? v[1] : e == 2 ? v[2] : v[3];
 }
 
-template <class T, class D, int K, int M>
-__global__ void __launch_bounds__(kNT, 1) k_vol(const VolKArgs<K> a) {
-  constexpr int RY = vol_ry<K, M>();
-  constexpr int TYO = vol_out_rows<K, M>();
+// MASK: zero taps that the pass skips are tested for (float input, where a
+// skipped tap keeps inf and nan out of the chain). Without it every tap takes
+// part: for finite inputs a zero tap leaves an FMA chain from +0 unchanged.
+template <class T, class D, int K, int M, int NW, bool MASK>
+__global__ void __launch_bounds__(32 * NW, 1) k_vol(const VolKArgs<K> a) {
+  constexpr int RY = vol_ry<K, M, NW>();
+  constexpr int TYO = vol_out_rows<K, M, NW>();
   constexpr int RXH = K / 2;  // x halo used by the x chain (symmetric taps)
   static_assert(RXH <= kHX, "x halo wider than one lane");
   constexpr int PF = vol_pf<T>();
   constexpr int DEPTH = PF + 1;
-  constexpr int SLOT = M * kNW * kRX;             // elements of T per prefetch slot
-  constexpr int PS = vol_plane_rows<K, M>() * kRX;  // floats per plane buffer
+  constexpr int SLOT = M * NW * kRX;             // elements of T per prefetch slot
+  constexpr int PS = vol_plane_rows<K, M, NW>() * kRX;  // floats per plane buffer
   extern __shared__ __align__(16) unsigned char sm_vol[];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  // this thread's prefetch position of group i: pre + slot * SLOT + i * kNW * kRX
+  // this thread's prefetch position of group i: pre + slot * SLOT + i * NW * kRX
   T* const pre = reinterpret_cast<T*>(sm_vol) + w * kRX + 4 * lane;
-  float* const P0 = reinterpret_cast<float*>(sm_vol + vol_pre_bytes<T, K, M>());
+  float* const P0 = reinterpret_cast<float*>(sm_vol + vol_pre_bytes<T, K, M, NW>());
 
   const int Z = a.Z, Y = a.Y, X = a.X;
   const long long YX = (long long)Y * X;
@@ -150,12 +159,12 @@ __global__ void __launch_bounds__(kNT, 1) k_vol(const VolKArgs<K> a) {
       }
     }
   }
-  // rows of this thread's groups: group i is region row w + kNW * i
+  // rows of this thread's groups: group i is region row w + NW * i
   int roff[M];         // mapped row * X + gx (read only by lanes inside the array)
   uint32_t rfill = 0;  // bit i: constant mode, row outside the array
 #pragma unroll
   for (int i = 0; i < M; ++i) {
-    const int gy = y0 - a.ay + w + kNW * i;
+    const int gy = y0 - a.ay + w + NW * i;
     const int my = (gy >= 0 && gy < Y) ? gy : map_coord32(gy, Y, a.my);
     roff[i] = my * X + gx;
     if (my < 0) rfill |= 1u << i;
@@ -183,7 +192,7 @@ __global__ void __launch_bounds__(kNT, 1) k_vol(const VolKArgs<K> a) {
           T* dst = pre + slot_w * SLOT;
 #pragma unroll
           for (int i = 0; i < M; ++i)
-            if (!((rfill >> i) & 1u)) fast::cp_async_vec4<T>(dst + i * kNW * kRX, src + roff[i]);
+            if (!((rfill >> i) & 1u)) fast::cp_async_vec4<T>(dst + i * NW * kRX, src + roff[i]);
         }
       }
       fast::cp_commit();
@@ -213,7 +222,7 @@ __global__ void __launch_bounds__(kNT, 1) k_vol(const VolKArgs<K> a) {
               if (mz < 0) {
                 v[0] = v[1] = pack2(cz, cz);
               } else if (col_in && !((rfill >> i) & 1u)) {
-                slot_to_pairs<T>(slot + i * kNW * kRX, v);
+                slot_to_pairs<T>(slot + i * NW * kRX, v);
               } else {
                 v[0] = v[1] = 0ull;
               }
@@ -222,14 +231,14 @@ __global__ void __launch_bounds__(kNT, 1) k_vol(const VolKArgs<K> a) {
               float* P = P0 + ((j - K + 1) & 1) * PS + w * kRX + 4 * lane;
 #pragma unroll
               for (int i = 0; i < M; ++i) {
-                float* pr = P + i * kNW * kRX;
+                float* pr = P + i * NW * kRX;
                 if ((rfill >> i) & 1u) {
                   *reinterpret_cast<float4*>(pr) = make_float4(cy, cy, cy, cy);
                 } else if (col_in) {
                   f2 acc[2] = {0ull, 0ull};
 #pragma unroll
                   for (int k = 0; k < K; ++k)
-                    if ((a.act_z >> k) & 1u) {
+                    if (!MASK || ((a.act_z >> k) & 1u)) {
                       acc[0] = fma2(win[i][(u + 1 + k) % K][0], a.wz2[k], acc[0]);
                       acc[1] = fma2(win[i][(u + 1 + k) % K][1], a.wz2[k], acc[1]);
                     }
@@ -257,7 +266,7 @@ __global__ void __launch_bounds__(kNT, 1) k_vol(const VolKArgs<K> a) {
 #pragma unroll
               for (int t = 0; t < M; ++t) {
                 const int k = rr - t;
-                if (k >= 0 && k < K && ((a.act_y >> k) & 1u)) {
+                if (k >= 0 && k < K && (!MASK || ((a.act_y >> k) & 1u))) {
                   q[t][0] = fma2(p.x, a.wy2[k], q[t][0]);
                   q[t][1] = fma2(p.y, a.wy2[k], q[t][1]);
                 }
@@ -279,7 +288,7 @@ __global__ void __launch_bounds__(kNT, 1) k_vol(const VolKArgs<K> a) {
               float xo[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
               for (int k = 0; k < K; ++k)
-                if ((a.act_x >> k) & 1u)
+                if (!MASK || ((a.act_x >> k) & 1u))
 #pragma unroll
                   for (int e = 0; e < 4; ++e) xo[e] = fmaf(xw[e + k], a.wx[k], xo[e]);
               if (t < nstore) fast::store4<D>(o + (long long)t * X, xo[0], xo[1], xo[2], xo[3]);
@@ -299,7 +308,7 @@ inline unsigned long long two_lanes(float w) {
   return (static_cast<unsigned long long>(b) << 32) | b;
 }
 
-template <class T, class D, int K, int M>
+template <class T, class D, int K, int M, int NW, bool MASK>
 int launch_vol_km(const VolArgs& v, cudaStream_t st) {
   VolKArgs<K> a{};
   a.in = v.in;
@@ -331,7 +340,7 @@ int launch_vol_km(const VolArgs& v, cudaStream_t st) {
     if (!(v.py.skip && v.py.w[k] == 0.f)) a.act_y |= 1u << k;
     if (!(v.px.skip && v.px.w[k] == 0.f)) a.act_x |= 1u << k;
   }
-  constexpr int TY = vol_out_rows<K, M>();
+  constexpr int TY = vol_out_rows<K, M, NW>();
   a.tiles_x = static_cast<int>((v.X + kTX - 1) / kTX);
   const long long tiles = (long long)a.tiles_x * ((v.Y + TY - 1) / TY);
   // z chunk: long enough that the K - 1 extra slices stay a small share,
@@ -341,27 +350,53 @@ int launch_vol_km(const VolArgs& v, cudaStream_t st) {
   a.zchunk = zc;
   const long long nzc = (v.Z + zc - 1) / zc;
   if (tiles > 0x7fffffffLL || nzc > 65535) return CIMX_FUSED_DECLINED;
-  constexpr size_t smem = vol_smem<T, K, M>();
+  constexpr size_t smem = vol_smem<T, K, M, NW>();
   static_assert(smem <= (size_t)fast::kMaxSmem, "volume kernel shared memory");
   static std::once_flag once;
   static cudaError_t attr = cudaSuccess;
   std::call_once(once, [] {
-    attr = cudaFuncSetAttribute(k_vol<T, D, K, M>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)smem);
+    attr = cudaFuncSetAttribute(k_vol<T, D, K, M, NW, MASK>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   });
   if (attr != cudaSuccess) return cuda_fail(attr, "volume kernel shared memory attribute");
   const dim3 grid((unsigned)tiles, (unsigned)nzc, (unsigned)std::min<long long>(v.B, 65535));
-  k_vol<T, D, K, M><<<grid, kNT, smem, st>>>(a);
+  k_vol<T, D, K, M, NW, MASK><<<grid, 32 * NW, smem, st>>>(a);
   return cuda_fail(cudaGetLastError(), "volume kernel launch");
 }
 
-// K = 3: four region rows per warp (62-row tiles); K = 5: three (44-row
-// tiles: the ring of five slices needs the registers)
+// Skipped zero taps only change a chain whose input is inf or nan. Integer
+// input is finite, and so is every intermediate while the taps cannot
+// overflow float32 (bounded here on the host) and the fill values are
+// finite: those launches run without the tests. Float input keeps them when
+// any pass skips a tap.
 template <class T, class D>
 int launch_vol_td(const VolArgs& v, cudaStream_t st) {
   const int K = v.pz.K;
-  if (K == 3) return launch_vol_km<T, D, 3, 4>(v, st);
-  if (K == 5) return launch_vol_km<T, D, 5, 3>(v, st);
+  bool mask = v.pz.skip || v.py.skip || v.px.skip;
+  auto nonfinite_fill = [](const SlabPass& p) {
+    return p.mode == CIMX_MODE_CONSTANT && !std::isfinite(p.cval);
+  };
+  if (mask && sizeof(T) < 4) {
+    if (nonfinite_fill(v.pz) || nonfinite_fill(v.py) || nonfinite_fill(v.px))
+      return CIMX_FUSED_DECLINED;
+    double sz = 0, sy = 0;
+    for (int k = 0; k < K; ++k) {
+      sz += std::fabs((double)v.pz.w[k]);
+      sy += std::fabs((double)v.py.w[k]);
+    }
+    // |z result| <= 65535 sz, |y result| <= 65535 sz sy (before rounding)
+    if (65536.0 * sz * std::max(1.0, sy) >= 1e37) return CIMX_FUSED_DECLINED;
+    mask = false;
+  }
+  if constexpr (sizeof(T) == 4) {
+    if (mask) {
+      if (K == 3) return launch_vol_km<T, D, 3, kM3, kNW, true>(v, st);
+      if (K == 5) return launch_vol_km<T, D, 5, kM5, kNW, true>(v, st);
+      return CIMX_FUSED_DECLINED;
+    }
+  }
+  if (K == 3) return launch_vol_km<T, D, 3, kM3, kNW, false>(v, st);
+  if (K == 5) return launch_vol_km<T, D, 5, kM5, kNW, false>(v, st);
   return CIMX_FUSED_DECLINED;
 }
 
