@@ -102,6 +102,33 @@ __device__ __forceinline__ void slot_to_pairs(const T* p, f2 (&v)[2]) {
   v[1] = pack2(fast::exact_float(q.z), fast::exact_float(q.w));
 }
 
+// cast<D>() of a chain result. TRUNC: the result is known (bounded on the
+// host) to lie in [0, max(D) + 1), where cast<D>() is truncation toward zero:
+// adding 2^23 rounded toward zero leaves the integer in the low mantissa bits.
+template <class D, bool TRUNC>
+__device__ __forceinline__ float vol_narrow(float a) {
+  if constexpr (sizeof(D) == 4) return a;
+  else if constexpr (TRUNC) return __fsub_rn(__fadd_rz(a, 8388608.0f), 8388608.0f);
+  else return fast::narrow_float<D>(a);
+}
+
+template <class D, bool TRUNC>
+__device__ __forceinline__ D vol_store_cast(float a) {
+  if constexpr (sizeof(D) < 4 && TRUNC)
+    return static_cast<D>(__float_as_uint(__fadd_rz(a, 8388608.0f)) & (sizeof(D) == 2 ? 0xFFFFu : 0xFFu));
+  else return out_cast<D>(a);
+}
+
+template <class D, bool TRUNC>
+__device__ __forceinline__ void vol_store4(D* p, float a, float b, float c, float d) {
+  typename fast::Vec4<D>::type q;
+  q.x = vol_store_cast<D, TRUNC>(a);
+  q.y = vol_store_cast<D, TRUNC>(b);
+  q.z = vol_store_cast<D, TRUNC>(c);
+  q.w = vol_store_cast<D, TRUNC>(d);
+  *reinterpret_cast<typename fast::Vec4<D>::type*>(p) = q;
+}
+
 __device__ __forceinline__ float pick4(const float (&v)[4], int e) {
   return e == 0 ? v[0] : e == 1 ? v[1] : e == 2 ? v[2] : v[3];
 }
@@ -109,7 +136,7 @@ __device__ __forceinline__ float pick4(const float (&v)[4], int e) {
 // MASK: zero taps that the pass skips are tested for (float input, where a
 // skipped tap keeps inf and nan out of the chain). Without it every tap takes
 // part: for finite inputs a zero tap leaves an FMA chain from +0 unchanged.
-template <class T, class D, int K, int M, int NW, bool MASK>
+template <class T, class D, int K, int M, int NW, bool MASK, bool TRUNC>
 __global__ void __launch_bounds__(32 * NW, 1) k_vol(const VolKArgs<K> a) {
   constexpr int RY = vol_ry<K, M, NW>();
   constexpr int TYO = vol_out_rows<K, M, NW>();
@@ -242,8 +269,8 @@ __global__ void __launch_bounds__(32 * NW, 1) k_vol(const VolKArgs<K> a) {
                       acc[0] = fma2(win[i][(u + 1 + k) % K][0], a.wz2[k], acc[0]);
                       acc[1] = fma2(win[i][(u + 1 + k) % K][1], a.wz2[k], acc[1]);
                     }
-                  float o[4] = {fast::narrow_float<D>(lo2(acc[0])), fast::narrow_float<D>(hi2(acc[0])),
-                                fast::narrow_float<D>(lo2(acc[1])), fast::narrow_float<D>(hi2(acc[1]))};
+                  float o[4] = {vol_narrow<D, TRUNC>(lo2(acc[0])), vol_narrow<D, TRUNC>(hi2(acc[0])),
+                                vol_narrow<D, TRUNC>(lo2(acc[1])), vol_narrow<D, TRUNC>(hi2(acc[1]))};
                   if (hc0 >= 0) {
                     pr[hc0 - 4 * lane] = pick4(o, he0);
                     if (hc1 >= 0) pr[hc1 - 4 * lane] = pick4(o, he1);
@@ -276,10 +303,10 @@ __global__ void __launch_bounds__(32 * NW, 1) k_vol(const VolKArgs<K> a) {
 #pragma unroll
             for (int t = 0; t < M; ++t) {
               float xw[4 + 2 * RXH];
-              xw[RXH + 0] = xfill ? cx : fast::narrow_float<D>(lo2(q[t][0]));
-              xw[RXH + 1] = xfill ? cx : fast::narrow_float<D>(hi2(q[t][0]));
-              xw[RXH + 2] = xfill ? cx : fast::narrow_float<D>(lo2(q[t][1]));
-              xw[RXH + 3] = xfill ? cx : fast::narrow_float<D>(hi2(q[t][1]));
+              xw[RXH + 0] = xfill ? cx : vol_narrow<D, TRUNC>(lo2(q[t][0]));
+              xw[RXH + 1] = xfill ? cx : vol_narrow<D, TRUNC>(hi2(q[t][0]));
+              xw[RXH + 2] = xfill ? cx : vol_narrow<D, TRUNC>(lo2(q[t][1]));
+              xw[RXH + 3] = xfill ? cx : vol_narrow<D, TRUNC>(hi2(q[t][1]));
 #pragma unroll
               for (int c = 0; c < RXH; ++c) {
                 xw[c] = __shfl_up_sync(0xffffffffu, xw[4 + c], 1);
@@ -291,7 +318,7 @@ __global__ void __launch_bounds__(32 * NW, 1) k_vol(const VolKArgs<K> a) {
                 if (!MASK || ((a.act_x >> k) & 1u))
 #pragma unroll
                   for (int e = 0; e < 4; ++e) xo[e] = fmaf(xw[e + k], a.wx[k], xo[e]);
-              if (t < nstore) fast::store4<D>(o + (long long)t * X, xo[0], xo[1], xo[2], xo[3]);
+              if (t < nstore) vol_store4<D, TRUNC>(o + (long long)t * X, xo[0], xo[1], xo[2], xo[3]);
             }
           }
           __syncthreads();
@@ -308,7 +335,7 @@ inline unsigned long long two_lanes(float w) {
   return (static_cast<unsigned long long>(b) << 32) | b;
 }
 
-template <class T, class D, int K, int M, int NW, bool MASK>
+template <class T, class D, int K, int M, int NW, bool MASK, bool TRUNC>
 int launch_vol_km(const VolArgs& v, cudaStream_t st) {
   VolKArgs<K> a{};
   a.in = v.in;
@@ -355,13 +382,40 @@ int launch_vol_km(const VolArgs& v, cudaStream_t st) {
   static std::once_flag once;
   static cudaError_t attr = cudaSuccess;
   std::call_once(once, [] {
-    attr = cudaFuncSetAttribute(k_vol<T, D, K, M, NW, MASK>,
+    attr = cudaFuncSetAttribute(k_vol<T, D, K, M, NW, MASK, TRUNC>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   });
   if (attr != cudaSuccess) return cuda_fail(attr, "volume kernel shared memory attribute");
   const dim3 grid((unsigned)tiles, (unsigned)nzc, (unsigned)std::min<long long>(v.B, 65535));
-  k_vol<T, D, K, M, NW, MASK><<<grid, 32 * NW, smem, st>>>(a);
+  k_vol<T, D, K, M, NW, MASK, TRUNC><<<grid, 32 * NW, smem, st>>>(a);
   return cuda_fail(cudaGetLastError(), "volume kernel launch");
+}
+
+// Integer input and integer output: when every tap is non-negative, every
+// fill value lies in [0, max(D)] and the largest input times the taps'
+// sums stays below max(D) + 1 after each pass, every chain result lies in
+// [0, max(D) + 1) and cast<D>() is plain truncation (the TRUNC kernels).
+template <class T, class D>
+bool trunc_bounded(const VolArgs& v) {
+  const double dmax = sizeof(D) == 2 ? 65535.0 : 255.0;
+  const double tmax = sizeof(T) == 2 ? 65535.0 : 255.0;
+  const SlabPass* ps[3] = {&v.pz, &v.py, &v.px};
+  double bound = tmax;
+  for (const SlabPass* p : ps) {
+    if (p->mode == CIMX_MODE_CONSTANT && !(p->cval >= 0.0 && p->cval <= std::min(tmax, dmax)))
+      return false;
+    double sum = 0.0;
+    for (int k = 0; k < p->K; ++k) {
+      if (!(p->w[k] >= 0.f)) return false;
+      sum += p->w[k];
+    }
+    // a float32 FMA chain of K non-negative terms exceeds the exact sum by
+    // at most K * 2^-24 of it (below 1e-6 for K <= 16); truncation only
+    // lowers the next pass's input
+    bound *= sum * (1.0 + 1e-6);
+    if (!(bound < dmax + 1.0)) return false;
+  }
+  return true;
 }
 
 // Skipped zero taps only change a chain whose input is inf or nan. Integer
@@ -390,13 +444,20 @@ int launch_vol_td(const VolArgs& v, cudaStream_t st) {
   }
   if constexpr (sizeof(T) == 4) {
     if (mask) {
-      if (K == 3) return launch_vol_km<T, D, 3, kM3, kNW, true>(v, st);
-      if (K == 5) return launch_vol_km<T, D, 5, kM5, kNW, true>(v, st);
+      if (K == 3) return launch_vol_km<T, D, 3, kM3, kNW, true, false>(v, st);
+      if (K == 5) return launch_vol_km<T, D, 5, kM5, kNW, true, false>(v, st);
       return CIMX_FUSED_DECLINED;
     }
   }
-  if (K == 3) return launch_vol_km<T, D, 3, kM3, kNW, false>(v, st);
-  if (K == 5) return launch_vol_km<T, D, 5, kM5, kNW, false>(v, st);
+  if constexpr (sizeof(T) < 4 && sizeof(D) < 4) {
+    if (trunc_bounded<T, D>(v)) {
+      if (K == 3) return launch_vol_km<T, D, 3, kM3, kNW, false, true>(v, st);
+      if (K == 5) return launch_vol_km<T, D, 5, kM5, kNW, false, true>(v, st);
+      return CIMX_FUSED_DECLINED;
+    }
+  }
+  if (K == 3) return launch_vol_km<T, D, 3, kM3, kNW, false, false>(v, st);
+  if (K == 5) return launch_vol_km<T, D, 5, kM5, kNW, false, false>(v, st);
   return CIMX_FUSED_DECLINED;
 }
 

@@ -61,6 +61,23 @@ def test_volume_uniform_u16_exact(ndi, mode, size, shape):
 
 
 @pytest.mark.parametrize("mode", MODES)
+@pytest.mark.parametrize("tin,tout", [(np.uint8, np.uint8), (np.uint8, np.uint16),
+                                      (np.uint16, np.uint16)])
+def test_volume_integer_smoothing(ndi, mode, tin, tout):
+    # non-negative taps on integer data: the truncating kernels
+    hi = 256 if tin == np.uint8 else 65536
+    x = _ints((7, 45, 132), tin, 4, hi=hi)
+    xd = dev(x)
+    for cval in (0.0, 200.0):
+        got = host(ndi.gaussian_filter(xd, 0.5, mode=mode, cval=cval, output=tout))
+        np.testing.assert_array_equal(got, R.gaussian_filter(x, 0.5, mode=mode, cval=cval,
+                                                             output=tout))
+        got = host(ndi.uniform_filter(xd, 3, mode=mode, cval=cval, output=tout))
+        np.testing.assert_array_equal(got, R.uniform_filter(x, 3, mode=mode, cval=cval,
+                                                            output=tout))
+
+
+@pytest.mark.parametrize("mode", MODES)
 @pytest.mark.parametrize("shape", [(9, 70, 128), (130, 20, 16), (3, 9, 8)])
 def test_volume_float_modes(ndi, mode, shape):
     x = np.random.default_rng(5).standard_normal(shape).astype(np.float32)
