@@ -1,9 +1,10 @@
-"""The single-launch 3-D kernel: a filter with 3 or 5 taps on each of the
-last three axes runs its z, y and x passes in one launch. Its outputs must be
-bit-identical to the oracle and to the pass-by-pass schedule (one launch per
-pass through a scratch volume). The shapes have rows of a multiple of 4
-elements (the kernel's condition) and cover partial tiles in y and x, short
-and chunked z, a leading batch axis and rows of only 8 elements."""
+"""The fused kernels of the plain path on rows of a multiple of 4 elements
+(the vector kernels' condition): the single-launch 3-D kernel (3 or 5 taps
+on each of the last three axes: z, y and x passes in one launch) and the
+(y, x) slab kernel with 9 or 17 taps. Their outputs must be bit-identical
+to the oracle and to the pass-by-pass schedule (one launch per pass through
+a scratch volume). The shapes cover partial tiles in y and x, short and
+chunked z, a leading batch axis and rows of only 8 elements."""
 
 import numpy as np
 import pytest
@@ -183,6 +184,38 @@ def test_out_of_range_fill_values(ndi, dtype, cval, shape):
     x = _ints(shape, dtype, 13, hi=200)
     got = host(ndi.uniform_filter(dev(x), 3, mode="constant", cval=cval))
     np.testing.assert_array_equal(got, R.uniform_filter(x, 3, mode="constant", cval=cval))
+
+
+@pytest.mark.parametrize("mode", MODES)
+@pytest.mark.parametrize("shape", [(300, 1000), (7, 130, 232), (5, 9, 8), (2, 3, 150, 116)])
+@pytest.mark.parametrize("sigma", [1.0, 2.0])
+def test_slab_long_taps_gaussian(ndi, mode, shape, sigma):
+    # 9 or 17 taps on the last two axes, with partial tiles in x and y,
+    # rows shorter than the taps and a batch axis
+    x = np.random.default_rng(21).standard_normal(shape).astype(np.float32)
+    axes = tuple(range(len(shape)))[-2:]
+    got = host(ndi.gaussian_filter(dev(x), sigma, mode=mode, cval=0.25, axes=axes))
+    exp = R.gaussian_filter(x, sigma, mode=mode, cval=0.25, axes=axes)
+    np.testing.assert_array_equal(got, exp)
+
+
+@pytest.mark.parametrize("tin,tout", [(np.uint16, np.float32), (np.uint8, np.uint8),
+                                      (np.uint16, np.uint16), (np.uint8, np.float32)])
+def test_slab_long_taps_dtypes(ndi, tin, tout):
+    x = _ints((3, 200, 360), tin, 22, hi=256 if tin == np.uint8 else 65536)
+    xd = dev(x)
+    for sigma, order in [((0, 2, 2), 0), ((0, 1, 1), 0), ((0, 2, 2), (0, 1, 0))]:
+        got = host(ndi.gaussian_filter(xd, sigma, order=order, mode="mirror", output=tout))
+        exp = R.gaussian_filter(x, sigma, order=order, mode="mirror", output=tout)
+        np.testing.assert_array_equal(got, exp)
+
+
+def test_slab_long_taps_match_pass_by_pass(ndi):
+    x = torch.rand((24, 1024, 1024), device="cuda")
+    got = ndi.gaussian_filter(x, (1, 2, 2), mode="mirror")
+    with ndi.pass_by_pass():
+        exp = ndi.gaussian_filter(x, (1, 2, 2), mode="mirror")
+    assert torch.equal(got, exp)
 
 
 def test_volume_status_clean(ndi):
