@@ -2,8 +2,9 @@
 // (cimx_fast.cuh, cimx_vol.cuh) and schedules them: a 3-D filter with short
 // taps on all three axes is one launch of the volume kernel (k_vol);
 // otherwise passes along leading axes are streamed one launch each
-// (k_stream), the passes along the last two axes run fused in one slab
-// launch (k_slab or k_rowstream). Intermediates follow cuCIM's _run_1d_filters
+// (k_stream; the generic kernel for taps it does not cover), the passes
+// along the last two axes run fused in one slab launch (k_slab or
+// k_rowstream). Intermediates follow cuCIM's _run_1d_filters
 // ping-pong: every pass writes the output dtype, the last launch writes the
 // caller's output, one scratch buffer takes the others.
 #include <algorithm>
@@ -161,11 +162,19 @@ int try_fused(const CimxArray* in, const CimxArray* out, PassDesc* ds, int npass
   for (int i = 0; i < npasses; ++i) (ds[i].axis < ylast ? lead : tail).push_back(i);
 
   std::vector<Trimmed> tr(npasses);
+  // a leading pass the stream kernel does not cover (longer taps, rows not
+  // a multiple of 4) runs on the generic kernel: worthwhile while the last
+  // two axes still take one slab launch
+  std::vector<char> lead_generic(npasses, 0);
   for (size_t n = 0; n < lead.size(); ++n) {
     const int i = lead[n];
     const int tin = n == 0 ? in->dtype : D;
-    if (!trim(ds[i], 17, tr[i]) || !stream_supports(tr[i].K)) return CIMX_FUSED_DECLINED;
-    if (!fast_pair(tin, D) || ds[i].inner % 4 != 0) return CIMX_FUSED_DECLINED;
+    const bool stream_ok = trim(ds[i], 17, tr[i]) && stream_supports(tr[i].K) &&
+                           fast_pair(tin, D) && ds[i].inner % 4 == 0;
+    if (!stream_ok) {
+      if (tail.empty()) return CIMX_FUSED_DECLINED;
+      lead_generic[i] = 1;
+    }
   }
   const int tail_in = lead.empty() ? in->dtype : D;
   if (!tail.empty()) {
@@ -196,7 +205,16 @@ int try_fused(const CimxArray* in, const CimxArray* out, PassDesc* ds, int npass
   int j = 0;
   for (int i : lead) {
     void* dst = dst_of(j++);
-    rc = launch_stream(ds[i], tr[i], tsrc, src, D, dst, st);
+    if (lead_generic[i]) {
+      PassDesc d = ds[i];
+      d.in = src;
+      d.out = dst;
+      d.tin = tsrc;
+      d.tout = D;
+      rc = launch_generic_pass(d, st);
+    } else {
+      rc = launch_stream(ds[i], tr[i], tsrc, src, D, dst, st);
+    }
     if (rc != CIMX_OK) break;
     src = dst;
     tsrc = D;

@@ -218,6 +218,20 @@ def test_slab_long_taps_match_pass_by_pass(ndi):
     assert torch.equal(got, exp)
 
 
+@pytest.mark.parametrize("mode", ["mirror", "constant", "wrap"])
+def test_long_leading_pass_then_slab(ndi, mode):
+    # the z pass is longer than the stream kernel takes (25 taps): it runs on
+    # the generic kernel, the (y, x) passes still as one slab launch
+    x = np.random.default_rng(23).standard_normal((30, 70, 136)).astype(np.float32)
+    xd = dev(x)
+    got = ndi.gaussian_filter(xd, (3.0, 2.0, 1.5), mode=mode, cval=0.5)
+    np.testing.assert_array_equal(host(got), R.gaussian_filter(x, (3.0, 2.0, 1.5), mode=mode,
+                                                               cval=0.5))
+    with ndi.pass_by_pass():
+        exp = ndi.gaussian_filter(xd, (3.0, 2.0, 1.5), mode=mode, cval=0.5)
+    assert torch.equal(got, exp)
+
+
 def test_volume_status_clean(ndi):
     from cucim_b200 import _lib
 
