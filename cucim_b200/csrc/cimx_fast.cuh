@@ -292,10 +292,6 @@ int launch_stream_td(const PassDesc& d, const float* w, int K, int anchor, bool 
 
 // ---------------------------------------------------------------- (b)
 
-// resident slab CTAs per SM asked of the compiler: four (64 registers a
-// thread) keep more tile loads in flight than three, which is what the
-// 74 registers a thread of the unconstrained build allowed
-constexpr int kSlabMinBlocks = 4;
 constexpr int kSlabTY = 32;    // output rows per tile
 constexpr int kSlabTX = 128;   // output columns per tile
 
@@ -328,13 +324,23 @@ struct Geom {
   static constexpr int MID = (kSlabTY / 2) * RXQ * 8;
   static constexpr int OFF_W = 128;
   static constexpr int RAWP = (RAW + 127) / 128 * 128;
-  // one TMA buffer: measured faster than two (two cost a resident CTA per SM)
+  // one TMA buffer: measured faster than two (two cost resident CTAs per SM;
+  // with two, the 17-tap gaussian of the 512 x 1024 x 1024 stack took
+  // 3.0 ms instead of 2.2 ms)
   static constexpr int NBUF = 1;
   static constexpr int OFF_A = OFF_W + 2 * KB * 8;  // raw (f32) or s_in
   static constexpr int SZ_A = F32 ? NBUF * RAWP : RY * RXS * 4;
   static constexpr int OFF_B = (OFF_A + SZ_A + 127) / 128 * 128;  // s_mid (f32) or union
   static constexpr int SZ_B = F32 ? MID : (RAW > MID ? RAW : MID);
   static constexpr int SMEM = OFF_B + SZ_B;
+  // threads: enough for every y-pass item (NPAIR column pairs x TY/P row
+  // groups) in one round; the x pass has TY/2 x TX/P = 256 items
+  static constexpr int NT = ((NPAIR * (kSlabTY / P) + 31) / 32) * 32;
+  static constexpr int NW = NT / 32;
+  // resident CTAs per SM asked of the compiler (registers per thread):
+  // three up to 320 threads (64 registers), two beyond (three would leave
+  // 56 registers and spill)
+  static constexpr int MINB = NT <= 320 ? 3 : 2;
 };
 
 __device__ __forceinline__ long long floor_div(long long a, long long b) {
@@ -455,7 +461,7 @@ __device__ __forceinline__ float staged_value(const T* in, long long gy, long lo
 }
 
 template <class T, class D, int KB, bool TMA>
-__global__ void __launch_bounds__(256, kSlabMinBlocks) k_slab(const __grid_constant__ CUtensorMap map,
+__global__ void __launch_bounds__(Geom<T, KB>::NT, Geom<T, KB>::MINB) k_slab(const __grid_constant__ CUtensorMap map,
                                                const SlabArgs a) {
   using G = Geom<T, KB>;
   extern __shared__ __align__(128) unsigned char smem[];
@@ -538,7 +544,7 @@ __global__ void __launch_bounds__(256, kSlabMinBlocks) k_slab(const __grid_const
     // outside the array with their boundary-mode values
     if (!(rl == 0 && rr == G::RY && cl == 0 && cr == G::RX)) {
       float* rawf = reinterpret_cast<float*>(raw);
-      for (int r = warp; r < G::RY; r += 8) {
+      for (int r = warp; r < G::RY; r += G::NW) {
         float* row = rawf + r * G::BX + off;
         if (r < rl || r >= rr) {
           for (int c = lane; c < G::RX; c += 32)
@@ -555,7 +561,7 @@ __global__ void __launch_bounds__(256, kSlabMinBlocks) k_slab(const __grid_const
     // convert to float into the staging buffer at column c (pairs aligned)
     float* dst = G::F32 ? reinterpret_cast<float*>(raw) : s_in;
     const int stride = G::F32 ? G::BX : G::RXS;
-    for (int r = warp; r < G::RY; r += 8) {
+    for (int r = warp; r < G::RY; r += G::NW) {
       const bool row_in = r >= rl && r < rr;
       for (int c = lane; c < G::RX; c += 32) {
         float v;
@@ -688,9 +694,9 @@ int launch_slab_kb(SlabArgs& a, cudaStream_t st) {
                    : std::min<long long>(a.B, 65535LL);
   const dim3 grid((unsigned)a.tiles_x, (unsigned)a.tiles_y, (unsigned)zs);
   if (tma)
-    k_slab<T, D, KB, true><<<grid, 256, G::SMEM, st>>>(map, a);
+    k_slab<T, D, KB, true><<<grid, G::NT, G::SMEM, st>>>(map, a);
   else
-    k_slab<T, D, KB, false><<<grid, 256, G::SMEM, st>>>(map, a);
+    k_slab<T, D, KB, false><<<grid, G::NT, G::SMEM, st>>>(map, a);
   return cuda_fail(cudaGetLastError(), "slab launch");
 }
 
