@@ -21,8 +21,11 @@ The 256 MiB image alone is above L2; every timed repetition reads it from HBM.
 
 Plain 2-D gaussian (reported in `plain_2d_gaussian`): gaussian sigma 4,
 truncate 4, mode 'reflect' on float32 2048 x 2048 uniform images (seed 0),
-16 distinct images per repetition so that the inputs exceed L2; GB/s at
-8 bytes per pixel and the fraction of the measured HBM copy bandwidth.
+16 distinct images per repetition so that the inputs exceed L2. The kernel
+rate (GB/s at 8 bytes per pixel, fraction of the measured HBM copy
+bandwidth) comes from one call over the 16 images as a stack; the per-call
+times of ndimage.gaussian_filter and skimage.filters.gaussian, one image per
+call, are reported beside it.
 
 Frangi (reported in `frangi`): skimage.filters.frangi(sigmas=1..5,
 alpha=beta=0.5, gamma=None, black_ridges=False) on the 256^3 float32
@@ -454,13 +457,25 @@ def run_plain2d(torch, dev, n_img=16, reps=5, hbm_gbs=None):
         for im, o in zip(imgs, outs):
             ndi.gaussian_filter(im, 4.0, mode="reflect", truncate=4.0, output=o)
 
+    # the same 16 images as one (16, 2048, 2048) stack filtered over axes
+    # (1, 2): one launch, no per-call host work -- the kernel's own rate
+    stack = torch.stack(imgs)
+    stack_out = torch.empty_like(stack)
+
+    def one_stack():
+        ndi.gaussian_filter(stack, 4.0, mode="reflect", truncate=4.0, axes=(1, 2), output=stack_out)
+
     ms = time_kernel(one_direct, reps, torch) / n_img
     ms_api = time_kernel(one, reps, torch) / n_img
-    gbs = 8 * base.numel() / (ms * 1e-3) / 1e9
+    ms_kernel = time_kernel(one_stack, reps, torch) / n_img
+    gbs = 8 * base.numel() / (ms_kernel * 1e-3) / 1e9
     res = {"workload": "float32 2048x2048 uniform (seed 0), gaussian sigma 4 (K=33), mode reflect; "
                        f"{n_img} distinct images per repetition (inputs above L2)",
-           "ms_per_image": ms, "gpx_s": base.numel() / (ms * 1e-3) / 1e9, "gb_s": gbs,
-           "ms_per_image_skimage_api": ms_api}
+           "ms_per_image_kernel": ms_kernel, "gpx_s": base.numel() / (ms_kernel * 1e-3) / 1e9,
+           "gb_s": gbs, "kernel_note": f"one launch over the {n_img} images as a stack, axes (1, 2)",
+           "ms_per_image_per_call": ms, "ms_per_image_skimage_api": ms_api,
+           "per_call_note": "one ndimage.gaussian_filter call per image (includes the host work "
+                            "of each call) and one skimage.filters.gaussian call per image"}
     if hbm_gbs:
         res["frac_of_hbm"] = gbs / hbm_gbs
     return res

@@ -153,7 +153,27 @@ def choose_algorithm(ndim, axis, K, anchor, mode, cval, in_dtype, algorithm=None
 
 
 def pass_flags(in_dtype, ndim, axis, K, origin, mode, cval, w_dtype, convolve, algorithm):
-    """CIMX_F_* flags for one pass."""
+    """CIMX_F_* flags for one pass (memoised: a pure function of its
+    arguments, called once per pass of every filter call)."""
+    try:
+        key = (np.dtype(in_dtype).str, ndim, axis, K, origin, mode, float(cval),
+               np.dtype(w_dtype).str, bool(convolve), algorithm)
+    except (TypeError, ValueError):
+        return _pass_flags(in_dtype, ndim, axis, K, origin, mode, cval, w_dtype, convolve,
+                           algorithm)
+    flags = _PASS_FLAGS.get(key)
+    if flags is None:
+        flags = _pass_flags(in_dtype, ndim, axis, K, origin, mode, cval, w_dtype, convolve,
+                            algorithm)
+        if len(_PASS_FLAGS) < 4096:
+            _PASS_FLAGS[key] = flags
+    return flags
+
+
+_PASS_FLAGS = {}
+
+
+def _pass_flags(in_dtype, ndim, axis, K, origin, mode, cval, w_dtype, convolve, algorithm):
     wdt = weights_dtype(in_dtype, w_dtype)
     o = origin
     if convolve:

@@ -115,8 +115,27 @@ def pass_by_pass():
         _EXTRA_LIB_FLAGS = old
 
 
-def _run(input, specs, output, cval, algorithm=None):
-    """Apply the pass list to `input` into `output` (FLT:363-396 semantics)."""
+def _hashable(obj):
+    """`obj` with lists turned into tuples, or None when it cannot be a key."""
+    if isinstance(obj, (list, tuple)):
+        items = tuple(_hashable(o) for o in obj)
+        return None if any(i is None and o is not None for i, o in zip(items, obj)) else items
+    try:
+        hash(obj)
+    except TypeError:
+        return None
+    return obj
+
+
+# Resolved pass lists (CimxPass arrays and the tap arrays they point into),
+# keyed by everything they depend on: repeated calls with the same filter
+# skip the tap arithmetic and the struct building.
+_PASS_CACHE = {}
+
+
+def _run(input, specs, output, cval, algorithm=None, cache_key=None):
+    """Apply the pass list to `input` into `output` (FLT:363-396 semantics).
+    `cache_key`: a hashable description of `specs` (None: not cached)."""
     x = _arrays.as_tensor(input)
     if x.dtype.is_complex:
         raise NotImplementedError("complex arrays are not supported")
@@ -126,11 +145,21 @@ def _run(input, specs, output, cval, algorithm=None):
     lib_flags = _EXTRA_LIB_FLAGS
     if algorithm in _TENSOR_FLAGS:
         lib_flags, algorithm = lib_flags | _TENSOR_FLAGS[algorithm], None
-    pl = _build_passes(_arrays.np_dtype(xc), out_dt, xc.dim(), specs, cval, algorithm)
-    arr = pl.array()
+    in_dt = _arrays.np_dtype(xc)
+    key = None
+    if cache_key is not None:
+        key = (cache_key, in_dt.str, np.dtype(out_dt).str, xc.dim(), _hashable(cval), algorithm)
+    hit = _PASS_CACHE.get(key) if key is not None else None
+    if hit is None:
+        pl = _build_passes(in_dt, out_dt, xc.dim(), specs() if callable(specs) else specs, cval,
+                           algorithm)
+        hit = (pl, pl.array(), len(pl))
+        if key is not None and len(_PASS_CACHE) < 1024:
+            _PASS_CACHE[key] = hit
+    _, arr, npasses = hit
     a_in = _arrays.to_cimx(xc)
     a_out = _arrays.to_cimx(slot.work)
-    rc = _lib.lib.cimx_separable(ctypes.byref(a_in), ctypes.byref(a_out), arr, len(pl),
+    rc = _lib.lib.cimx_separable(ctypes.byref(a_in), ctypes.byref(a_out), arr, npasses,
                                  lib_flags, _arrays.stream_of(xc))
     _lib.check(rc, "separable filter")
     return slot.result()
@@ -200,14 +229,34 @@ def uniform_filter(input, size=3, output=None, mode="reflect", cval=0.0, origin=
     origins = _util.fix_sequence_arg(origin, n, "origin", int)
     modes = _util.fix_sequence_arg(mode, n, "mode", _util.check_mode)
     wdt = np.promote_types(_arrays.np_dtype(x), np.float32)
-    specs = [(ax, np.full(s, 1 / s, dtype=wdt), m, o, False)
-             for ax, s, m, o in zip(axes, sizes, modes, origins) if s > 1]
-    return _run(input, specs, output, cval, algorithm)
+
+    def specs():
+        return [(ax, np.full(s, 1 / s, dtype=wdt), m, o, False)
+                for ax, s, m, o in zip(axes, sizes, modes, origins) if s > 1]
+
+    key = _hashable(("uniform", tuple(axes), tuple(sizes), tuple(modes), tuple(origins)))
+    return _run(input, specs, output, cval, algorithm, cache_key=key)
 
 
 # ------------------------------------------------------------- gaussian
 
+_TAPS = {}
+
+
 def _gaussian_kernel1d(sigma, order, radius, dtype=np.float64):
+    """Memoised _gaussian_taps (read-only arrays: the taps of a sigma, order,
+    radius and dtype never change)."""
+    key = (float(sigma), int(order), int(radius), np.dtype(dtype).str)
+    w = _TAPS.get(key)
+    if w is None:
+        w = _gaussian_taps(sigma, order, radius, dtype)
+        w.setflags(write=False)
+        if len(_TAPS) < 4096:
+            _TAPS[key] = w
+    return w
+
+
+def _gaussian_taps(sigma, order, radius, dtype=np.float64):
     """Gaussian (derivative) correlation taps, FLT:689-717.
 
     Order 0: the normalised exp(-x^2 / (2 sigma^2)) in float64 (returned as
@@ -271,11 +320,13 @@ def gaussian_filter(input, sigma, order=0, output=None, mode="reflect", cval=0.0
                     truncate=4.0, radius=None, axes=None, *, algorithm=None):
     """Multi-dimensional Gaussian filter (FLT:580-686)."""
     x = _arrays.as_tensor(input)
-    specs = _gaussian_specs(x.dim(), _arrays.np_dtype(x), sigma, order, mode, truncate,
-                            radius, axes)
-    if specs is None:
-        specs = []
-    return _run(input, specs, output, cval, algorithm)
+
+    def specs():
+        return _gaussian_specs(x.dim(), _arrays.np_dtype(x), sigma, order, mode, truncate,
+                               radius, axes) or []
+
+    key = _hashable(("gaussian", sigma, order, mode, truncate, radius, axes))
+    return _run(input, specs, output, cval, algorithm, cache_key=key)
 
 
 def gaussian_filter1d(input, sigma, axis=-1, order=0, output=None, mode="reflect", cval=0.0,
@@ -295,11 +346,15 @@ def _prewitt_or_sobel(input, axis, output, mode, cval, smooth, algorithm):
     x = _arrays.as_tensor(input)
     axis = _util.normalize_axis(axis, x.dim())
     wdt = np.promote_types(_arrays.np_dtype(x), np.float32)
-    diff = np.array([-1, 0, 1], dtype=wdt)
-    specs = [(a, diff if a == axis else smooth, mode, 0, False) for a in range(x.dim())]
-    for m in {mode}:
-        _util.check_mode(m)
-    return _run(input, specs, output, cval, algorithm)
+    _util.check_mode(mode)
+
+    def specs():
+        diff = np.array([-1, 0, 1], dtype=wdt)
+        return [(a, diff if a == axis else smooth, mode, 0, False) for a in range(x.dim())]
+
+    key = _hashable(("prewitt_or_sobel", axis, mode, tuple(np.asarray(smooth).tolist()),
+                     np.asarray(smooth).dtype.str))
+    return _run(input, specs, output, cval, algorithm, cache_key=key)
 
 
 def sobel(input, axis=-1, output=None, mode="reflect", cval=0.0, *, algorithm=None):
