@@ -99,6 +99,10 @@ _sigs = {
     "cimx_gradient_magnitude": (
         [_A, _A, _P(CimxPass), ctypes.c_int, ctypes.c_int, ctypes.c_void_p], ctypes.c_int,
     ),
+    "cimx_laplace": (
+        [_A, _A, _P(CimxPass), ctypes.c_int, ctypes.c_int, ctypes.c_void_p], ctypes.c_int,
+    ),
+    "cimx_combine": ([_A, _A, ctypes.c_int, ctypes.c_void_p], ctypes.c_int),
     "cimx_eigvals_sym": (
         [_A, ctypes.c_int, _A, ctypes.c_int, ctypes.c_int, ctypes.c_void_p], ctypes.c_int,
     ),
@@ -122,6 +126,9 @@ for _name, (_args, _res) in _sigs.items():
     _fn.restype = _res
 
 EXPORTED = tuple(_sigs)
+
+COMBINE_ADD = 0
+COMBINE_SUBTRACT = 1
 
 
 def last_error():

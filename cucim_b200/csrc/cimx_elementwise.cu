@@ -9,6 +9,8 @@
 #include <cmath>
 #include <vector>
 
+#include <type_traits>
+
 #include "cimx_common.cuh"
 #include "cimx_fused.h"
 #include "cimx_internal.h"
@@ -56,6 +58,52 @@ __global__ void k_square_acc(F* acc, const F* t, int64_t n, int first) {
       const double sq = __dmul_rn(t[i], t[i]);
       acc[i] = first ? sq : __dadd_rn(acc[i], sq);
     }
+  }
+}
+
+// acc = acc + t or acc - t in acc's dtype, as CuPy's `output += tmp`
+// (_vendored/_ndimage_filters.py:888, generic_laplace) and `out -= ...`
+// (filters/_gaussian.py:164, difference_of_gaussians) compute it: integers
+// wrap around, floats round to nearest.
+template <class T>
+__global__ void k_combine(T* acc, const T* t, int64_t n, int sub) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    if constexpr (std::is_same<T, float>::value) {
+      acc[i] = sub ? __fsub_rn(acc[i], t[i]) : __fadd_rn(acc[i], t[i]);
+    } else if constexpr (std::is_same<T, double>::value) {
+      acc[i] = sub ? __dsub_rn(acc[i], t[i]) : __dadd_rn(acc[i], t[i]);
+    } else if constexpr (std::is_same<T, __half>::value) {
+      acc[i] = sub ? __hsub(acc[i], t[i]) : __hadd(acc[i], t[i]);
+    } else {
+      using U = typename std::make_unsigned<T>::type;
+      using W = typename std::conditional<(sizeof(T) < 4), uint32_t, U>::type;
+      const W a = static_cast<W>(static_cast<U>(acc[i])), b = static_cast<W>(static_cast<U>(t[i]));
+      acc[i] = static_cast<T>(static_cast<U>(sub ? a - b : a + b));
+    }
+  }
+}
+
+template <class T>
+int launch_combine_t(void* acc, const void* t, int64_t n, int sub, cudaStream_t st) {
+  k_combine<T><<<grid_for(n), 256, 0, st>>>(static_cast<T*>(acc), static_cast<const T*>(t), n, sub);
+  return cuda_fail(cudaGetLastError(), "combine launch");
+}
+
+int launch_combine(void* acc, const void* t, int dt, int64_t n, int sub, cudaStream_t st) {
+  switch (dt) {
+    case DT_F32: return launch_combine_t<float>(acc, t, n, sub, st);
+    case DT_F64: return launch_combine_t<double>(acc, t, n, sub, st);
+    case DT_F16: return launch_combine_t<__half>(acc, t, n, sub, st);
+    case DT_U8: return launch_combine_t<uint8_t>(acc, t, n, sub, st);
+    case DT_I8: return launch_combine_t<int8_t>(acc, t, n, sub, st);
+    case DT_U16: return launch_combine_t<uint16_t>(acc, t, n, sub, st);
+    case DT_I16: return launch_combine_t<int16_t>(acc, t, n, sub, st);
+    case DT_U32: return launch_combine_t<uint32_t>(acc, t, n, sub, st);
+    case DT_I32: return launch_combine_t<int32_t>(acc, t, n, sub, st);
+    case DT_U64: case DT_U64Q: return launch_combine_t<unsigned long long>(acc, t, n, sub, st);
+    case DT_I64: case DT_I64Q: return launch_combine_t<long long>(acc, t, n, sub, st);
+    default: return fail(CIMX_E_DTYPE, "combine: unsupported dtype");
   }
 }
 
@@ -404,6 +452,45 @@ int cimx_gradient_magnitude(const CimxArray* in, const CimxArray* out, const Cim
       rc = launch_square_accumulate(out->data, dst->data, out->dtype, n, a == 0, st);
   }
   if (rc == CIMX_OK) rc = launch_sqrt_inplace(out->data, out->dtype, n, st);
+  scratch_free(tmp, bytes, st);
+  return rc;
+}
+
+int cimx_combine(const CimxArray* acc, const CimxArray* term, int op, void* stream) {
+  if (!acc || !term || (op != CIMX_COMBINE_ADD && op != CIMX_COMBINE_SUBTRACT))
+    return fail(CIMX_E_INVALID, "bad combine arguments");
+  if (acc->dtype != term->dtype) return fail(CIMX_E_DTYPE, "combine: dtypes differ");
+  if (!same_shape(acc, term)) return fail(CIMX_E_INVALID, "combine: shapes differ");
+  if (!contiguous(acc) || !contiguous(term))
+    return fail(CIMX_E_LAYOUT, "combine: arrays must be C-contiguous");
+  const int64_t n = numel(acc);
+  if (n == 0) return CIMX_OK;
+  return launch_combine(acc->data, term->data, acc->dtype, n, op == CIMX_COMBINE_SUBTRACT,
+                        static_cast<cudaStream_t>(stream));
+}
+
+int cimx_laplace(const CimxArray* in, const CimxArray* out, const CimxPass* passes, int naxes,
+                 int passes_per_axis, void* stream) {
+  if (!in || !out || !passes || naxes < 1 || passes_per_axis < 0)
+    return fail(CIMX_E_INVALID, "bad laplace arguments");
+  if (!same_shape(in, out)) return fail(CIMX_E_INVALID, "output shape not correct");
+  if (!contiguous(out)) return fail(CIMX_E_LAYOUT, "output is not C-contiguous");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const int64_t n = numel(out);
+  if (n == 0) return CIMX_OK;
+  const size_t bytes = (size_t)n * dtype_size(out->dtype);
+  void* tmp = nullptr;
+  if (naxes > 1) {
+    tmp = scratch_alloc(bytes, st);
+    if (!tmp) return fail(CIMX_E_NOMEM, "scratch allocation for laplace failed");
+  }
+  CimxArray t = *out;
+  t.data = tmp;
+  int rc = cimx_separable(in, out, passes, passes_per_axis, 0, stream);
+  for (int a = 1; a < naxes && rc == CIMX_OK; ++a) {
+    rc = cimx_separable(in, &t, passes + (size_t)a * passes_per_axis, passes_per_axis, 0, stream);
+    if (rc == CIMX_OK) rc = launch_combine(out->data, tmp, out->dtype, n, 0, st);
+  }
   scratch_free(tmp, bytes, st);
   return rc;
 }

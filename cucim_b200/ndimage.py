@@ -22,6 +22,7 @@ __all__ = [
     "correlate1d", "convolve1d", "uniform_filter1d", "uniform_filter",
     "gaussian_filter1d", "gaussian_filter", "prewitt", "sobel",
     "generic_gradient_magnitude", "gaussian_gradient_magnitude",
+    "generic_laplace", "laplace", "gaussian_laplace",
 ]
 
 
@@ -397,6 +398,120 @@ def _gradient_magnitude(input, chains, output, cval, algorithm=None):
                                           len(chains), lens.pop(), _arrays.stream_of(xc))
     _lib.check(rc, "gradient magnitude")
     return slot.result()
+
+
+def _combine(acc, term, op):
+    """acc (+|-)= term in acc's dtype (libcimx; integers wrap)."""
+    a_acc, a_t = _arrays.to_cimx(acc), _arrays.to_cimx(term)
+    rc = _lib.lib.cimx_combine(ctypes.byref(a_acc), ctypes.byref(a_t), op,
+                               _arrays.stream_of(acc))
+    _lib.check(rc, "combine")
+
+
+def _laplace_sum(input, chains, output, cval, algorithm=None):
+    """sum over chains of chain(input), accumulated in the output dtype
+    (FLT:806-890 with the derivative of each axis a pass chain)."""
+    x = _arrays.as_tensor(input)
+    xc = x.contiguous()
+    slot = _arrays.output_slot(output, input, xc)
+    out_dt = slot.dtype
+    lens = {len(c) for c in chains}
+    if len(lens) != 1:
+        raise RuntimeError("laplace chains must have equal length")
+    if algorithm in _TENSOR_FLAGS:
+        algorithm = None  # the composite runs the plain passes
+    pl = _PassList()
+    for chain in chains:
+        sub = _build_passes(_arrays.np_dtype(xc), out_dt, xc.dim(), chain, cval, algorithm)
+        pl.keep += sub.keep
+        pl.items += sub.items
+    arr = pl.array()
+    a_in = _arrays.to_cimx(xc)
+    a_out = _arrays.to_cimx(slot.work)
+    rc = _lib.lib.cimx_laplace(ctypes.byref(a_in), ctypes.byref(a_out), arr, len(chains),
+                               lens.pop(), _arrays.stream_of(xc))
+    _lib.check(rc, "laplace")
+    return slot.result()
+
+
+def generic_laplace(input, derivative2, output=None, mode="reflect", cval=0.0,
+                    extra_arguments=(), extra_keywords=None, *, axes=None):
+    """FLT:806-890 with a user-supplied second-derivative callable: the
+    first axis into `output`, every further axis into one temporary of the
+    output dtype that is added in place (in libcimx, integers wrap)."""
+    if extra_keywords is None:
+        extra_keywords = {}
+    x = _arrays.as_tensor(input)
+    axes = _util.check_axes(axes, x.dim())
+    n = len(axes)
+    slot = _arrays.output_slot(output, input, x.contiguous())
+    if n == 0:
+        # elementwise copy with conversion: an empty pass list
+        _run(input, [], slot.work, cval)
+        return slot.result()
+    modes = _util.fix_sequence_arg(mode, n, "mode", _util.check_mode)
+
+    def into(res, dst):
+        r = _arrays.as_tensor(res)
+        if r.data_ptr() != dst.data_ptr():
+            dst.copy_(r)
+
+    into(derivative2(input, axes[0], slot.work, modes[0], cval, *extra_arguments,
+                     **extra_keywords), slot.work)
+    if n > 1:
+        tmp = torch.empty_like(slot.work)
+        for i in range(1, n):
+            into(derivative2(input, axes[i], tmp, modes[i], cval, *extra_arguments,
+                             **extra_keywords), tmp)
+            _combine(slot.work, tmp, _lib.COMBINE_ADD)
+    return slot.result()
+
+
+def laplace(input, output=None, mode="reflect", cval=0.0, *, axes=None, algorithm=None):
+    """Laplace filter from [1, -2, 1] second differences (FLT:893-930): one
+    correlate1d per axis, summed in the output dtype."""
+    x = _arrays.as_tensor(input)
+    axes = _util.check_axes(axes, x.dim())
+    if not axes:
+        return generic_laplace(input, None, output, mode, cval, axes=axes)
+    modes = _util.fix_sequence_arg(mode, len(axes), "mode", _util.check_mode)
+    wdt = np.promote_types(_arrays.np_dtype(x), np.float32)
+    w = np.array([1, -2, 1], dtype=wdt)
+    chains = [[(ax, w, m, 0, False)] for ax, m in zip(axes, modes)]
+    return _laplace_sum(input, chains, output, cval, algorithm)
+
+
+def gaussian_laplace(input, sigma, output=None, mode="reflect", cval=0.0, *, axes=None,
+                     algorithm=None, **kwargs):
+    """Laplace filter from Gaussian second derivatives (FLT:933-1009): per
+    filtered axis a gaussian_filter with order 2 on that axis (sigma 0 on the
+    axes not filtered) in that axis' mode, summed in the output dtype."""
+    x = _arrays.as_tensor(input)
+    ndim = x.dim()
+    axes = _util.check_axes(axes, ndim)
+    if not axes:
+        return generic_laplace(input, None, output, mode, cval, axes=axes)
+    n = len(axes)
+    sigmas = _util.fix_sequence_arg(sigma, n, "sigma", float)
+    if n < ndim:
+        full = [0.0] * ndim
+        for s_, ax in zip(sigmas, axes):
+            full[ax] = s_
+        sigmas = full
+    modes = _util.fix_sequence_arg(mode, n, "mode", _util.check_mode)
+    truncate = kwargs.pop("truncate", 4.0)
+    radius = kwargs.pop("radius", None)
+    if kwargs:
+        raise TypeError(f"unexpected keyword arguments {sorted(kwargs)}")
+    chains = []
+    for ax, m in zip(axes, modes):
+        order = [0] * ndim
+        order[ax] = 2
+        specs = _gaussian_specs(ndim, _arrays.np_dtype(x), sigmas, order, m, truncate, radius,
+                                None)
+        chains.append(specs if specs is not None else [])
+    # every chain drops the same zero-sigma axes, so the chains have equal length
+    return _laplace_sum(input, chains, output, cval, algorithm)
 
 
 def generic_gradient_magnitude(input, derivative, output=None, mode="reflect", cval=0.0,

@@ -15,7 +15,7 @@ from .._util import check_mode, supported_float_type
 from . import util as _u
 from .feature import _hessian_matrix_with_gaussian, symmetric_compute_eigenvalues
 
-__all__ = ["gaussian", "sobel", "prewitt", "frangi"]
+__all__ = ["gaussian", "difference_of_gaussians", "sobel", "prewitt", "frangi"]
 
 
 def gaussian(image, sigma=1, mode="nearest", cval=0, preserve_range=False, truncate=4.0, *,
@@ -48,6 +48,39 @@ def gaussian(image, sigma=1, mode="nearest", cval=0, preserve_range=False, trunc
 
 _SOBEL_SMOOTH = np.array([1, 2, 1]) / 4
 _PREWITT_SMOOTH = np.full((3,), 1 / 3)
+
+
+def difference_of_gaussians(image, low_sigma, high_sigma=None, *, mode="nearest", cval=0,
+                            channel_axis=None, truncate=4.0):
+    """filters/_gaussian.py:13-174: img_as_float, then gaussian(low_sigma)
+    minus gaussian(high_sigma) (high_sigma defaults to 1.6 low_sigma), the
+    subtraction in place in the float dtype (libcimx)."""
+    image = _u.img_as_float(image)
+    x = _arrays.as_tensor(image)
+    spatial_dims = x.dim() - 1 if channel_axis is not None else x.dim()
+    if np.isscalar(low_sigma):
+        low_sigma = (low_sigma,) * spatial_dims
+    low_sigma = tuple(map(float, low_sigma))
+    if high_sigma is None:
+        high_sigma = tuple(low * 1.6 for low in low_sigma)
+    elif np.isscalar(high_sigma):
+        high_sigma = (high_sigma,) * spatial_dims
+    high_sigma = tuple(map(float, high_sigma))
+    if len(low_sigma) != 1 and len(low_sigma) != spatial_dims:
+        raise ValueError("low_sigma must have length equal to number of"
+                         " spatial dimensions of input")
+    if len(high_sigma) != 1 and len(high_sigma) != spatial_dims:
+        raise ValueError("high_sigma must have length equal to number of"
+                         " spatial dimensions of input")
+    if any(s_hi < s_low for s_hi, s_low in zip(high_sigma, low_sigma)):
+        raise ValueError("high_sigma must be equal to or larger thanlow_sigma for all axes")
+    out = gaussian(image, sigma=low_sigma, mode=mode, cval=cval, channel_axis=channel_axis,
+                   truncate=truncate, preserve_range=False)
+    high = gaussian(image, sigma=high_sigma, mode=mode, cval=cval, channel_axis=channel_axis,
+                    truncate=truncate, preserve_range=False)
+    out_t = _arrays.as_tensor(out)
+    ndi._combine(out_t, _arrays.as_tensor(high).contiguous(), _lib.COMBINE_SUBTRACT)
+    return out
 
 
 def _generic_edge_filter(image, *, smooth_weights, edge_weights=(1, 0, -1), axis=None,

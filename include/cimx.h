@@ -170,6 +170,24 @@ CIMX_API int cimx_gradient_magnitude(const CimxArray* in, const CimxArray* out,
                             const CimxPass* passes, int naxes, int passes_per_axis,
                             void* stream);
 
+/* Laplacian as a sum of per-axis chains: out = chain_0(in), then
+ * tmp = chain_a(in); out += tmp (in out's dtype) for a >= 1. `passes` holds
+ * naxes chains of passes_per_axis passes each (axis a's chain at
+ * passes + a * passes_per_axis). Replaces generic_laplace as driven by
+ * laplace and gaussian_laplace (_vendored/_ndimage_filters.py:806-1009: one
+ * correlate1d with [1, -2, 1], or one gaussian_filter with order 2 on the
+ * axis, per axis). */
+CIMX_API int cimx_laplace(const CimxArray* in, const CimxArray* out, const CimxPass* passes,
+                          int naxes, int passes_per_axis, void* stream);
+
+/* acc = acc + term (op CIMX_COMBINE_ADD) or acc - term (CIMX_COMBINE_SUBTRACT)
+ * in acc's dtype: integers wrap, floats round to nearest. Both arrays have
+ * the same dtype and shape and are C-contiguous. The in-place `output += tmp`
+ * of generic_laplace (_vendored/_ndimage_filters.py:888) and `out -= ...` of
+ * difference_of_gaussians (filters/_gaussian.py:164). */
+enum { CIMX_COMBINE_ADD = 0, CIMX_COMBINE_SUBTRACT = 1 };
+CIMX_API int cimx_combine(const CimxArray* acc, const CimxArray* term, int op, void* stream);
+
 /* Closed-form eigenvalues of symmetric 2x2 / 3x3 matrices given as the
  * upper-triangular element images in row-major order ((00,01,11) or
  * (00,01,02,11,12,22)). `out` holds nelems==3 ? 2 : 3 images of the same

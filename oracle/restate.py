@@ -483,6 +483,85 @@ def sk_gaussian(image, sigma=1, mode="nearest", cval=0, preserve_range=False,
     return res
 
 
+def generic_laplace(input, derivative2, output=None, mode="reflect", cval=0.0,
+                    extra_arguments=(), extra_keywords=None, *, axes=None):
+    """FLT:806-890: derivative2 along the first axis into the output, every
+    further axis into a temporary of the output dtype added in place (numpy
+    add in that dtype: integers wrap, floats round to nearest)."""
+    input = np.asarray(input)
+    if extra_keywords is None:
+        extra_keywords = {}
+    axes = check_axes(axes, input.ndim)
+    out = get_output(output, input)
+    if len(axes) == 0:
+        out[...] = input
+        return out
+    modes = fix_sequence_arg(mode, len(axes), "mode", check_mode)
+    out[...] = derivative2(input, axes[0], out, modes[0], cval, *extra_arguments,
+                           **extra_keywords)
+    if len(axes) > 1:
+        tmp = np.empty_like(out)
+        for i in range(1, len(axes)):
+            tmp[...] = derivative2(input, axes[i], tmp, modes[i], cval, *extra_arguments,
+                                   **extra_keywords)
+            np.add(out, tmp, out=out)
+    return out
+
+
+def laplace(input, output=None, mode="reflect", cval=0.0, *, axes=None, algorithm=None):
+    """FLT:893-930: correlate1d with [1, -2, 1] per axis, summed."""
+    input = np.asarray(input)
+    w = np.array([1, -2, 1], dtype=np.promote_types(input.dtype, np.float32))
+
+    def derivative2(inp, axis, out, m, c):
+        return correlate1d(inp, w, axis, out, m, c, algorithm=algorithm)
+
+    return generic_laplace(input, derivative2, output, mode, cval, axes=axes)
+
+
+def gaussian_laplace(input, sigma, output=None, mode="reflect", cval=0.0, *, axes=None,
+                     algorithm=None, **kwargs):
+    """FLT:933-1009: per axis a gaussian_filter with order 2 on that axis
+    (sigma 0 on the axes not filtered), summed."""
+    input = np.asarray(input)
+    axes = check_axes(axes, input.ndim)
+    n = len(axes)
+    sigma = fix_sequence_arg(sigma, n, "sigma", float)
+    if n < input.ndim:
+        full = [0] * input.ndim
+        for s_, ax in zip(sigma, axes):
+            full[ax] = s_
+        sigma = full
+
+    def derivative2(inp, axis, out, m, c, sig, **kw):
+        order = [0] * inp.ndim
+        order[axis] = 2
+        return gaussian_filter(inp, sig, order, out, m, c, algorithm=algorithm, **kw)
+
+    return generic_laplace(input, derivative2, output, mode, cval, extra_arguments=(sigma,),
+                           extra_keywords=kwargs, axes=axes)
+
+
+def difference_of_gaussians(image, low_sigma, high_sigma=None, *, mode="nearest", cval=0,
+                            channel_axis=None, truncate=4.0):
+    """filters/_gaussian.py:13-174."""
+    image = img_as_float(image)
+    spatial_dims = image.ndim - 1 if channel_axis is not None else image.ndim
+    if np.isscalar(low_sigma):
+        low_sigma = (low_sigma,) * spatial_dims
+    low_sigma = tuple(map(float, low_sigma))
+    if high_sigma is None:
+        high_sigma = tuple(low * 1.6 for low in low_sigma)
+    elif np.isscalar(high_sigma):
+        high_sigma = (high_sigma,) * spatial_dims
+    high_sigma = tuple(map(float, high_sigma))
+    out = sk_gaussian(image, sigma=low_sigma, mode=mode, cval=cval, channel_axis=channel_axis,
+                      truncate=truncate)
+    out -= sk_gaussian(image, sigma=high_sigma, mode=mode, cval=cval,
+                       channel_axis=channel_axis, truncate=truncate)
+    return out
+
+
 _SOBEL_SMOOTH = np.array([1, 2, 1]) / 4
 _PREWITT_SMOOTH = np.full((3,), 1 / 3)
 

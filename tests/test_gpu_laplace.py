@@ -1,0 +1,116 @@
+"""laplace, gaussian_laplace, generic_laplace (FLT:806-1009) and skimage's
+difference_of_gaussians (filters/_gaussian.py:13-174): bit for bit against
+the oracle (per-axis chains of the separable kernels, summed in the output
+dtype: integers wrap)."""
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import restate as R
+
+pytestmark = pytest.mark.gpu
+
+MODES = ["reflect", "mirror", "nearest", "wrap", "constant"]
+
+
+def dev(a):
+    return torch.as_tensor(np.ascontiguousarray(a)).cuda()
+
+
+def host(t):
+    return t.cpu().numpy()
+
+
+@pytest.fixture(scope="module")
+def ndi(cuda):
+    from cucim_b200 import ndimage
+
+    return ndimage
+
+
+@pytest.fixture(scope="module")
+def ski(cuda):
+    from cucim_b200 import skimage
+
+    return skimage
+
+
+def _data(shape, dtype, seed=31):
+    rng = np.random.default_rng(seed)
+    dt = np.dtype(dtype)
+    if dt.kind in "iu":
+        return rng.integers(0, 200, shape).astype(dt)
+    return rng.standard_normal(shape).astype(dt)
+
+
+@pytest.mark.parametrize("mode", MODES)
+@pytest.mark.parametrize("dtype", [np.float32, np.float64, np.uint8, np.uint16, np.int16])
+@pytest.mark.parametrize("shape", [(40, 57), (9, 20, 24), (300,)])
+def test_laplace(ndi, mode, dtype, shape):
+    x = _data(shape, dtype)
+    got = host(ndi.laplace(dev(x), mode=mode, cval=3.0))
+    np.testing.assert_array_equal(got, R.laplace(x, mode=mode, cval=3.0))
+
+
+def test_laplace_axes_output_and_empty_axes(ndi):
+    x = _data((12, 18, 20), np.uint8)
+    xd = dev(x)
+    got = host(ndi.laplace(xd, output=np.float32, axes=(0, 2), mode=("mirror", "nearest")))
+    exp = R.laplace(x, output=np.float32, axes=(0, 2), mode=("mirror", "nearest"))
+    np.testing.assert_array_equal(got, exp)
+    got = host(ndi.laplace(xd, output=np.uint16, axes=()))
+    np.testing.assert_array_equal(got, R.laplace(x, output=np.uint16, axes=()))
+
+
+@pytest.mark.parametrize("mode", MODES)
+@pytest.mark.parametrize("sigma", [1.0, (0.8, 2.0, 1.3), 3.0])
+def test_gaussian_laplace(ndi, mode, sigma):
+    x = _data((14, 33, 40), np.float32)
+    got = host(ndi.gaussian_laplace(dev(x), sigma, mode=mode, cval=-1.0))
+    np.testing.assert_array_equal(got, R.gaussian_laplace(x, sigma, mode=mode, cval=-1.0))
+
+
+def test_gaussian_laplace_axes_dtypes_kwargs(ndi):
+    x = _data((10, 30, 36), np.uint16)
+    xd = dev(x)
+    got = host(ndi.gaussian_laplace(xd, (1.5, 2.0), axes=(1, 2), output=np.float32,
+                                    truncate=3.0))
+    exp = R.gaussian_laplace(x, (1.5, 2.0), axes=(1, 2), output=np.float32, truncate=3.0)
+    np.testing.assert_array_equal(got, exp)
+    got = host(ndi.gaussian_laplace(xd, 1.0, output=np.int16))
+    np.testing.assert_array_equal(got, R.gaussian_laplace(x, 1.0, output=np.int16))
+
+
+def test_generic_laplace_user_callable(ndi):
+    x = _data((25, 31), np.float32)
+    w = np.array([0.5, -1.25, 0.75], dtype=np.float32)
+
+    def d2(inp, axis, out, mode, cval, scale=1.0):
+        return ndi.correlate1d(inp, w * scale, axis, out, mode, cval)
+
+    def d2_ref(inp, axis, out, mode, cval, scale=1.0):
+        return R.correlate1d(inp, w * scale, axis, out, mode, cval)
+
+    got = host(ndi.generic_laplace(dev(x), d2, mode="nearest", extra_keywords={"scale": 2.0}))
+    exp = R.generic_laplace(x, d2_ref, mode="nearest", extra_keywords={"scale": 2.0})
+    np.testing.assert_array_equal(got, exp)
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.uint8, np.float64])
+def test_difference_of_gaussians(ski, dtype):
+    x = _data((48, 64), dtype)
+    got = host(ski.filters.difference_of_gaussians(dev(x), 1.5))
+    np.testing.assert_array_equal(got, R.difference_of_gaussians(x, 1.5))
+    got = host(ski.filters.difference_of_gaussians(dev(x), (1.0, 2.0), (2.0, 5.0),
+                                                   mode="reflect"))
+    exp = R.difference_of_gaussians(x, (1.0, 2.0), (2.0, 5.0), mode="reflect")
+    np.testing.assert_array_equal(got, exp)
+
+
+def test_difference_of_gaussians_channels_and_errors(ski):
+    x = _data((30, 40, 3), np.uint8)
+    got = host(ski.filters.difference_of_gaussians(dev(x), 1.0, channel_axis=-1))
+    np.testing.assert_array_equal(got, R.difference_of_gaussians(x, 1.0, channel_axis=-1))
+    with pytest.raises(ValueError):
+        ski.filters.difference_of_gaussians(dev(x), 2.0, 1.0, channel_axis=-1)

@@ -298,3 +298,17 @@ def test_frangi_small_oracle_properties():
     np.testing.assert_array_equal(R.frangi(z, sigmas=[1, 2]), 0)
     v = R.frangi(np.random.default_rng(2).random((20, 21)).astype(np.float32), sigmas=[1, 2])
     assert v.dtype == np.float32 and np.all((v >= 0) & (v <= 1))
+
+
+@pytest.mark.parametrize("mode", ["reflect", "mirror", "nearest", "constant", "wrap"])
+def test_laplace_family_matches_scipy_float64(mode):
+    # the oracle's laplace and gaussian_laplace (FLT:806-1009) in float64
+    # agree with scipy.ndimage up to the order of the final sums
+    import scipy.ndimage as sndi
+
+    x = np.random.default_rng(5).standard_normal((16, 21, 19))
+    np.testing.assert_allclose(R.laplace(x, mode=mode, cval=0.5),
+                               sndi.laplace(x, mode=mode, cval=0.5), rtol=0, atol=1e-12)
+    np.testing.assert_allclose(R.gaussian_laplace(x, (1.5, 0.7, 2.0), mode=mode, cval=0.5),
+                               sndi.gaussian_laplace(x, (1.5, 0.7, 2.0), mode=mode, cval=0.5),
+                               rtol=0, atol=1e-12)
