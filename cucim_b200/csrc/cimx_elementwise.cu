@@ -107,6 +107,35 @@ int launch_combine(void* acc, const void* t, int dt, int64_t n, int sub, cudaStr
   }
 }
 
+// filters/_unsharp_mask.py:12-20: result = image + (image - blurred) * amount,
+// each operation a separate CuPy kernel (rounded on its own, no contraction),
+// then cp.clip(result, lo, hi) when a range is given (nan passes through).
+template <class F>
+__global__ void k_unsharp(const F* __restrict__ img, const F* __restrict__ blur, F* out,
+                          int64_t n, F amount, int clip, F lo, F hi) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    F r;
+    if constexpr (sizeof(F) == 4) {
+      r = __fadd_rn(img[i], __fmul_rn(__fsub_rn(img[i], blur[i]), amount));
+    } else {
+      r = __dadd_rn(img[i], __dmul_rn(__dsub_rn(img[i], blur[i]), amount));
+    }
+    if (clip) r = r < lo ? lo : (r > hi ? hi : r);
+    out[i] = r;
+  }
+}
+
+// any element < 0 (filters/_unsharp_mask.py:145, cp.any(fimg < 0))
+template <class F>
+__global__ void k_any_negative(const F* __restrict__ a, int64_t n, int* flag) {
+  int found = 0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    found |= a[i] < F(0);
+  if (__syncthreads_or(found) && threadIdx.x == 0) atomicOr(flag, 1);
+}
+
 template <class F>
 __global__ void k_sqrt(F* acc, int64_t n) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
@@ -467,6 +496,58 @@ int cimx_combine(const CimxArray* acc, const CimxArray* term, int op, void* stre
   if (n == 0) return CIMX_OK;
   return launch_combine(acc->data, term->data, acc->dtype, n, op == CIMX_COMBINE_SUBTRACT,
                         static_cast<cudaStream_t>(stream));
+}
+
+int cimx_unsharp(const CimxArray* image, const CimxArray* blurred, const CimxArray* out,
+                 double amount, int clip, double lo, double hi, void* stream) {
+  if (!image || !blurred || !out) return fail(CIMX_E_INVALID, "bad unsharp arguments");
+  const int dt = image->dtype;
+  if (dt != DT_F32 && dt != DT_F64) return fail(CIMX_E_DTYPE, "unsharp: float32 or float64");
+  if (blurred->dtype != dt || out->dtype != dt) return fail(CIMX_E_DTYPE, "unsharp: dtypes differ");
+  if (!same_shape(image, blurred) || !same_shape(image, out))
+    return fail(CIMX_E_INVALID, "unsharp: shapes differ");
+  if (!contiguous(image) || !contiguous(blurred) || !contiguous(out))
+    return fail(CIMX_E_LAYOUT, "unsharp: arrays must be C-contiguous");
+  const int64_t n = numel(out);
+  if (n == 0) return CIMX_OK;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (dt == DT_F32)
+    k_unsharp<float><<<grid_for(n), 256, 0, st>>>(
+        static_cast<const float*>(image->data), static_cast<const float*>(blurred->data),
+        static_cast<float*>(out->data), n, static_cast<float>(amount), clip,
+        static_cast<float>(lo), static_cast<float>(hi));
+  else
+    k_unsharp<double><<<grid_for(n), 256, 0, st>>>(
+        static_cast<const double*>(image->data), static_cast<const double*>(blurred->data),
+        static_cast<double*>(out->data), n, amount, clip, lo, hi);
+  return cuda_fail(cudaGetLastError(), "unsharp launch");
+}
+
+int cimx_any_negative(const CimxArray* a, int* result, void* stream) {
+  if (!a || !result) return fail(CIMX_E_INVALID, "bad any_negative arguments");
+  if (a->dtype != DT_F32 && a->dtype != DT_F64)
+    return fail(CIMX_E_DTYPE, "any_negative: float32 or float64");
+  if (!contiguous(a)) return fail(CIMX_E_LAYOUT, "any_negative: array must be C-contiguous");
+  *result = 0;
+  const int64_t n = numel(a);
+  if (n == 0) return CIMX_OK;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  int* flag = static_cast<int*>(scratch_alloc(sizeof(int), st));
+  if (!flag) return fail(CIMX_E_NOMEM, "scratch allocation for any_negative failed");
+  int rc = cuda_fail(cudaMemsetAsync(flag, 0, sizeof(int), st), "any_negative memset");
+  if (rc == CIMX_OK) {
+    if (a->dtype == DT_F32)
+      k_any_negative<float><<<grid_for(n), 256, 0, st>>>(static_cast<const float*>(a->data), n, flag);
+    else
+      k_any_negative<double><<<grid_for(n), 256, 0, st>>>(static_cast<const double*>(a->data), n, flag);
+    rc = cuda_fail(cudaGetLastError(), "any_negative launch");
+  }
+  if (rc == CIMX_OK)
+    rc = cuda_fail(cudaMemcpyAsync(result, flag, sizeof(int), cudaMemcpyDeviceToHost, st),
+                   "any_negative readback");
+  if (rc == CIMX_OK) rc = cuda_fail(cudaStreamSynchronize(st), "any_negative synchronize");
+  scratch_free(flag, sizeof(int), st);
+  return rc;
 }
 
 int cimx_laplace(const CimxArray* in, const CimxArray* out, const CimxPass* passes, int naxes,

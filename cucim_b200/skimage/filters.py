@@ -15,7 +15,7 @@ from .._util import check_mode, supported_float_type
 from . import util as _u
 from .feature import _hessian_matrix_with_gaussian, symmetric_compute_eigenvalues
 
-__all__ = ["gaussian", "difference_of_gaussians", "sobel", "prewitt", "frangi"]
+__all__ = ["gaussian", "difference_of_gaussians", "unsharp_mask", "sobel", "prewitt", "frangi"]
 
 
 def gaussian(image, sigma=1, mode="nearest", cval=0, preserve_range=False, truncate=4.0, *,
@@ -81,6 +81,48 @@ def difference_of_gaussians(image, low_sigma, high_sigma=None, *, mode="nearest"
     out_t = _arrays.as_tensor(out)
     ndi._combine(out_t, _arrays.as_tensor(high).contiguous(), _lib.COMBINE_SUBTRACT)
     return out
+
+
+def _unsharp_mask_single_channel(image, radius, amount, vrange):
+    """filters/_unsharp_mask.py:12-20: the gaussian blur (mode 'reflect'),
+    then image + (image - blurred) * amount and the clip in one kernel."""
+    img = _arrays.as_tensor(image).contiguous()
+    blurred = _arrays.as_tensor(gaussian(img, sigma=radius, mode="reflect")).contiguous()
+    out = torch.empty_like(img)
+    a_img, a_bl, a_out = _arrays.to_cimx(img), _arrays.to_cimx(blurred), _arrays.to_cimx(out)
+    clip, lo, hi = (0, 0.0, 0.0) if vrange is None else (1, float(vrange[0]), float(vrange[1]))
+    rc = _lib.lib.cimx_unsharp(ctypes.byref(a_img), ctypes.byref(a_bl), ctypes.byref(a_out),
+                               float(amount), clip, lo, hi, _arrays.stream_of(img))
+    _lib.check(rc, "unsharp mask")
+    return out
+
+
+def unsharp_mask(image, radius=1.0, amount=1.0, preserve_range=False, *, channel_axis=None):
+    """filters/_unsharp_mask.py:23-160: float conversion (img_as_float unless
+    preserve_range), the clip range [-1, 1] or [0, 1] from whether any value
+    is negative (a device reduction and one readback, as cp.any is), and the
+    per-channel loop for channel_axis."""
+    x = _arrays.as_tensor(image)
+    float_dtype = supported_float_type(_arrays.np_dtype(x))
+    vrange = None
+    if preserve_range:
+        fimg = _arrays.as_tensor(_u.astype(image, float_dtype))
+    else:
+        fimg = _arrays.as_tensor(_u.astype(_u.img_as_float(image), float_dtype)).contiguous()
+        flag = ctypes.c_int(0)
+        a = _arrays.to_cimx(fimg)
+        rc = _lib.lib.cimx_any_negative(ctypes.byref(a), ctypes.byref(flag),
+                                        _arrays.stream_of(fimg))
+        _lib.check(rc, "unsharp mask range")
+        vrange = [-1.0, 1.0] if flag.value else [0.0, 1.0]
+    if channel_axis is not None:
+        result = torch.empty_like(fimg)
+        ax = channel_axis % fimg.dim()
+        for c in range(fimg.shape[ax]):
+            sl = tuple(c if d == ax else slice(None) for d in range(fimg.dim()))
+            result[sl] = _unsharp_mask_single_channel(fimg[sl], radius, amount, vrange)
+        return _arrays.wrap_like(image, result)
+    return _arrays.wrap_like(image, _unsharp_mask_single_channel(fimg, radius, amount, vrange))
 
 
 def _generic_edge_filter(image, *, smooth_weights, edge_weights=(1, 0, -1), axis=None,

@@ -188,6 +188,17 @@ CIMX_API int cimx_laplace(const CimxArray* in, const CimxArray* out, const CimxP
 enum { CIMX_COMBINE_ADD = 0, CIMX_COMBINE_SUBTRACT = 1 };
 CIMX_API int cimx_combine(const CimxArray* acc, const CimxArray* term, int op, void* stream);
 
+/* out = image + (image - blurred) * amount, each operation rounded on its
+ * own, then clipped to [lo, hi] when `clip` (nan passes through): the
+ * elementwise part of skimage's unsharp mask (filters/_unsharp_mask.py:12-20).
+ * float32 or float64, equal dtypes and shapes, C-contiguous. */
+CIMX_API int cimx_unsharp(const CimxArray* image, const CimxArray* blurred, const CimxArray* out,
+                          double amount, int clip, double lo, double hi, void* stream);
+
+/* *result = 1 when some element of `a` (float32/float64) is below zero, else 0;
+ * waits for the stream (filters/_unsharp_mask.py:145, cp.any(fimg < 0)). */
+CIMX_API int cimx_any_negative(const CimxArray* a, int* result, void* stream);
+
 /* Closed-form eigenvalues of symmetric 2x2 / 3x3 matrices given as the
  * upper-triangular element images in row-major order ((00,01,11) or
  * (00,01,02,11,12,22)). `out` holds nelems==3 ? 2 : 3 images of the same

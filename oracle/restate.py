@@ -562,6 +562,37 @@ def difference_of_gaussians(image, low_sigma, high_sigma=None, *, mode="nearest"
     return out
 
 
+def unsharp_mask(image, radius=1.0, amount=1.0, preserve_range=False, *, channel_axis=None):
+    """filters/_unsharp_mask.py:12-160."""
+    image = np.asarray(image)
+    float_dtype = supported_float_type(image.dtype)
+    vrange = None
+    if preserve_range:
+        fimg = image.astype(float_dtype, copy=False)
+    else:
+        fimg = img_as_float(image).astype(float_dtype, copy=False)
+        vrange = [-1.0, 1.0] if np.any(fimg < 0) else [0.0, 1.0]
+
+    def single(img):
+        img = np.ascontiguousarray(img)
+        blurred = sk_gaussian(img, sigma=radius, mode="reflect")
+        amt = img.dtype.type(amount)
+        result = img + (img - blurred) * amt
+        if vrange is not None:
+            lo, hi = img.dtype.type(vrange[0]), img.dtype.type(vrange[1])
+            result = np.where(result < lo, lo, np.where(result > hi, hi, result))
+        return result.astype(img.dtype, copy=False)
+
+    if channel_axis is not None:
+        result = np.empty_like(fimg, dtype=float_dtype)
+        ax = channel_axis % fimg.ndim
+        for c in range(image.shape[ax]):
+            sl = tuple(c if d == ax else slice(None) for d in range(fimg.ndim))
+            result[sl] = single(fimg[sl])
+        return result
+    return single(fimg)
+
+
 _SOBEL_SMOOTH = np.array([1, 2, 1]) / 4
 _PREWITT_SMOOTH = np.full((3,), 1 / 3)
 

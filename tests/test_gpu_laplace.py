@@ -1,7 +1,8 @@
 """laplace, gaussian_laplace, generic_laplace (FLT:806-1009) and skimage's
-difference_of_gaussians (filters/_gaussian.py:13-174): bit for bit against
-the oracle (per-axis chains of the separable kernels, summed in the output
-dtype: integers wrap)."""
+difference_of_gaussians (filters/_gaussian.py:13-174) and unsharp_mask
+(filters/_unsharp_mask.py:12-160): bit for bit against the oracle (per-axis
+chains of the separable kernels, summed in the output dtype: integers wrap;
+the unsharp combination rounded operation by operation)."""
 
 import numpy as np
 import pytest
@@ -114,3 +115,22 @@ def test_difference_of_gaussians_channels_and_errors(ski):
     np.testing.assert_array_equal(got, R.difference_of_gaussians(x, 1.0, channel_axis=-1))
     with pytest.raises(ValueError):
         ski.filters.difference_of_gaussians(dev(x), 2.0, 1.0, channel_axis=-1)
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.uint8, np.float64, np.int16])
+@pytest.mark.parametrize("radius,amount", [(1.0, 1.0), (2.5, 0.7), (0.5, 3.0)])
+def test_unsharp_mask(ski, dtype, radius, amount):
+    x = _data((40, 52), dtype)
+    got = host(ski.filters.unsharp_mask(dev(x), radius, amount))
+    np.testing.assert_array_equal(got, R.unsharp_mask(x, radius, amount))
+
+
+def test_unsharp_mask_preserve_range_and_channels(ski):
+    x = _data((24, 30, 3), np.uint8)
+    got = host(ski.filters.unsharp_mask(dev(x), 2.0, 1.5, channel_axis=-1))
+    np.testing.assert_array_equal(got, R.unsharp_mask(x, 2.0, 1.5, channel_axis=-1))
+    got = host(ski.filters.unsharp_mask(dev(x), 1.0, 2.0, preserve_range=True))
+    np.testing.assert_array_equal(got, R.unsharp_mask(x, 1.0, 2.0, preserve_range=True))
+    xf = _data((24, 30), np.float32)  # negative values: clip to [-1, 1]
+    got = host(ski.filters.unsharp_mask(dev(xf), 1.0, 1.0))
+    np.testing.assert_array_equal(got, R.unsharp_mask(xf, 1.0, 1.0))
