@@ -109,6 +109,11 @@ _sigs = {
         ctypes.c_int,
     ),
     "cimx_any_negative": ([_A, _P(ctypes.c_int), ctypes.c_void_p], ctypes.c_int),
+    "cimx_min_max_1d": (
+        [_A, _A, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+         ctypes.c_int, ctypes.c_void_p],
+        ctypes.c_int,
+    ),
     "cimx_eigvals_sym": (
         [_A, ctypes.c_int, _A, ctypes.c_int, ctypes.c_int, ctypes.c_void_p], ctypes.c_int,
     ),

@@ -23,6 +23,7 @@ __all__ = [
     "gaussian_filter1d", "gaussian_filter", "prewitt", "sobel",
     "generic_gradient_magnitude", "gaussian_gradient_magnitude",
     "generic_laplace", "laplace", "gaussian_laplace",
+    "minimum_filter1d", "maximum_filter1d",
 ]
 
 
@@ -512,6 +513,38 @@ def gaussian_laplace(input, sigma, output=None, mode="reflect", cval=0.0, *, axe
         chains.append(specs if specs is not None else [])
     # every chain drops the same zero-sigma axes, so the chains have equal length
     return _laplace_sum(input, chains, output, cval, algorithm)
+
+
+def _min_or_max_1d(input, size, axis, output, mode, cval, origin, is_max):
+    """FLT:1412-1448: one launch of libcimx's min/max kernel."""
+    x = _arrays.as_tensor(input)
+    if x.dtype.is_complex:
+        raise NotImplementedError("complex arrays are not supported")
+    size = int(size)
+    if size < 1:
+        raise RuntimeError("incorrect filter size")
+    axis = _util.normalize_axis(axis, x.dim())
+    origin = _util.check_origin(origin, size)
+    mode = "grid-wrap" if mode == "wrap" else mode
+    _util.check_mode(mode)
+    xc = x.contiguous()
+    slot = _arrays.output_slot(output, input, xc)
+    a_in, a_out = _arrays.to_cimx(xc), _arrays.to_cimx(slot.work)
+    rc = _lib.lib.cimx_min_max_1d(ctypes.byref(a_in), ctypes.byref(a_out), size, axis, origin,
+                                  _lib.MODE_CODES[mode], float(cval), 1 if is_max else 0,
+                                  _arrays.stream_of(xc))
+    _lib.check(rc, "min/max filter")
+    return slot.result()
+
+
+def minimum_filter1d(input, size, axis=-1, output=None, mode="reflect", cval=0.0, origin=0):
+    """Minimum over `size` elements along `axis` (FLT:1362-1385)."""
+    return _min_or_max_1d(input, size, axis, output, mode, cval, origin, False)
+
+
+def maximum_filter1d(input, size, axis=-1, output=None, mode="reflect", cval=0.0, origin=0):
+    """Maximum over `size` elements along `axis` (FLT:1388-1411)."""
+    return _min_or_max_1d(input, size, axis, output, mode, cval, origin, True)
 
 
 def generic_gradient_magnitude(input, derivative, output=None, mode="reflect", cval=0.0,

@@ -199,6 +199,14 @@ CIMX_API int cimx_unsharp(const CimxArray* image, const CimxArray* blurred, cons
  * waits for the stream (filters/_unsharp_mask.py:145, cp.any(fimg < 0)). */
 CIMX_API int cimx_any_negative(const CimxArray* a, int* result, void* stream);
 
+/* minimum_filter1d (is_max 0) / maximum_filter1d (is_max 1) of `size`
+ * elements along `axis` (_vendored/_ndimage_filters.py:1362-1497): the
+ * element itself, then the window in order, folded with fmin / fmax in
+ * double (nan-ignoring); cval (as a double) outside the array in constant
+ * mode; cast<D>() on store. C-contiguous arrays of any real dtype. */
+CIMX_API int cimx_min_max_1d(const CimxArray* in, const CimxArray* out, int size, int axis,
+                             int origin, int mode, double cval, int is_max, void* stream);
+
 /* Closed-form eigenvalues of symmetric 2x2 / 3x3 matrices given as the
  * upper-triangular element images in row-major order ((00,01,11) or
  * (00,01,02,11,12,22)). `out` holds nelems==3 ? 2 : 3 images of the same

@@ -293,3 +293,23 @@ void oracle_cast(const void* in, int w64, void* out, int tout, int64_t n) {
     store_cast(out, tout, i, a, w64);
   }
 }
+
+/* minimum_filter1d / maximum_filter1d (_vendored/_ndimage_filters.py:1362-1497,
+ * _get_min_or_max_kernel without weights): value = x[l] as a double, then
+ * every window element in order folded with fmin / fmax (cval outside the
+ * array in constant mode), stored with cast<D>(). */
+void oracle_min_max1d(const void* in, int tin, void* out, int tout, int64_t outer, int64_t L,
+                      int64_t inner, int size, int anchor, int mode, double cval, int is_max) {
+  for (int64_t o = 0; o < outer; ++o)
+    for (int64_t l = 0; l < L; ++l)
+      for (int64_t i = 0; i < inner; ++i) {
+        const int64_t base = o * L * inner + i;
+        double value = load_d(in, tin, base + l * inner);
+        for (int k = 0; k < size; ++k) {
+          const int64_t m = map_index(l - anchor + k, L, mode);
+          const double v = m < 0 ? cval : load_d(in, tin, base + m * inner);
+          value = is_max ? fmax(v, value) : fmin(v, value);
+        }
+        store_cast(out, tout, base + l * inner, value, 1);
+      }
+}

@@ -35,6 +35,12 @@ _lib.oracle_cast.argtypes = [
     ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int64,
 ]
 _lib.oracle_cast.restype = None
+_lib.oracle_min_max1d.argtypes = [
+    ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
+    ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+    ctypes.c_double, ctypes.c_int,
+]
+_lib.oracle_min_max1d.restype = None
 
 MODES = {
     "reflect": 0, "grid-mirror": 0, "mirror": 1, "nearest": 2,
@@ -481,6 +487,38 @@ def sk_gaussian(image, sigma=1, mode="nearest", cval=0, preserve_range=False,
         out[...] = res
         return out
     return res
+
+
+def _min_or_max_1d(input, size, axis, output, mode, cval, origin, is_max):
+    """FLT:1412-1497 (min/max kernel without weights) in the C oracle."""
+    input = np.ascontiguousarray(np.asarray(input))
+    size = int(size)
+    if size < 1:
+        raise RuntimeError("incorrect filter size")
+    axis = axis % input.ndim
+    origin = check_origin(origin, size)
+    mode = "grid-wrap" if mode == "wrap" else mode
+    check_mode(mode)
+    out = get_output(output, input)
+    res = np.empty(input.shape, out.dtype)
+    shape = input.shape
+    outer = int(np.prod(shape[:axis], dtype=np.int64))
+    inner = int(np.prod(shape[axis + 1:], dtype=np.int64))
+    _lib.oracle_min_max1d(input.ctypes.data, ord(input.dtype.char), res.ctypes.data,
+                          ord(res.dtype.char), outer, shape[axis], inner, size,
+                          size // 2 + origin, MODES[mode], float(cval), int(is_max))
+    out[...] = res
+    return out
+
+
+def minimum_filter1d(input, size, axis=-1, output=None, mode="reflect", cval=0.0, origin=0):
+    """FLT:1362-1385."""
+    return _min_or_max_1d(input, size, axis, output, mode, cval, origin, False)
+
+
+def maximum_filter1d(input, size, axis=-1, output=None, mode="reflect", cval=0.0, origin=0):
+    """FLT:1388-1411."""
+    return _min_or_max_1d(input, size, axis, output, mode, cval, origin, True)
 
 
 def generic_laplace(input, derivative2, output=None, mode="reflect", cval=0.0,

@@ -1,8 +1,10 @@
-"""laplace, gaussian_laplace, generic_laplace (FLT:806-1009) and skimage's
-difference_of_gaussians (filters/_gaussian.py:13-174) and unsharp_mask
-(filters/_unsharp_mask.py:12-160): bit for bit against the oracle (per-axis
-chains of the separable kernels, summed in the output dtype: integers wrap;
-the unsharp combination rounded operation by operation)."""
+"""The rest of the separable family: laplace, gaussian_laplace,
+generic_laplace (FLT:806-1009), minimum_filter1d / maximum_filter1d
+(FLT:1362-1497) and skimage's difference_of_gaussians
+(filters/_gaussian.py:13-174) and unsharp_mask (filters/_unsharp_mask.py:
+12-160): bit for bit against the oracle (per-axis chains of the separable
+kernels, summed in the output dtype: integers wrap; the unsharp combination
+rounded operation by operation; min / max folded in double)."""
 
 import numpy as np
 import pytest
@@ -134,3 +136,39 @@ def test_unsharp_mask_preserve_range_and_channels(ski):
     xf = _data((24, 30), np.float32)  # negative values: clip to [-1, 1]
     got = host(ski.filters.unsharp_mask(dev(xf), 1.0, 1.0))
     np.testing.assert_array_equal(got, R.unsharp_mask(xf, 1.0, 1.0))
+
+
+
+@pytest.mark.parametrize("mode", MODES)
+@pytest.mark.parametrize("dtype", [np.float32, np.uint8, np.uint16, np.int16, np.float64])
+@pytest.mark.parametrize("shape", [(33, 47), (6, 20, 25), (500,)])
+def test_min_max_filter1d(ndi, mode, dtype, shape):
+    x = _data(shape, dtype)
+    xd = dev(x)
+    for axis in range(len(shape)):
+        for size, origin in [(1, 0), (3, 0), (4, 1), (9, -3), (40, 2)]:
+            for name in ("minimum_filter1d", "maximum_filter1d"):
+                got = host(getattr(ndi, name)(xd, size, axis, mode=mode, cval=5.0,
+                                              origin=origin))
+                exp = getattr(R, name)(x, size, axis, mode=mode, cval=5.0, origin=origin)
+                np.testing.assert_array_equal(got, exp)
+
+
+def test_min_max_filter1d_nan_outputs_and_errors(ndi):
+    x = _data((20, 30), np.float32)
+    x[3, 4] = np.nan
+    x[10, :] = np.nan  # a row of nan: nan survives only where the window is all nan
+    xd = dev(x)
+    for name in ("minimum_filter1d", "maximum_filter1d"):
+        for axis in (0, 1):
+            got = host(getattr(ndi, name)(xd, 5, axis))
+            np.testing.assert_array_equal(got, getattr(R, name)(x, 5, axis))
+        got = host(getattr(ndi, name)(dev(_data((20, 30), np.uint8)), 4, 0, output=np.int16,
+                                      mode="constant", cval=300.0))
+        exp = getattr(R, name)(_data((20, 30), np.uint8), 4, 0, output=np.int16,
+                               mode="constant", cval=300.0)
+        np.testing.assert_array_equal(got, exp)
+    with pytest.raises(RuntimeError):
+        ndi.minimum_filter1d(xd, 0)
+    with pytest.raises(ValueError):
+        ndi.minimum_filter1d(xd, 3, origin=2)
