@@ -215,4 +215,31 @@ __host__ __device__ __forceinline__ int map_coord32(int ix, int n, int mode) {
   }
 }
 
+// map_coord with the common case first: an overhang of at most one axis
+// length (every tap window shorter than the axis) needs one reflection or
+// shift, computed without a division; longer ones take map_coord's periodic
+// formula. The same index as map_coord. For code that maps many elements
+// (tile borders, generic passes); the streaming kernels keep the plain
+// map_coord, whose smaller inlined body suits their per-row loops.
+__host__ __device__ __forceinline__ int64_t map_coord_near(int64_t ix, int64_t n, int mode) {
+  if (ix >= 0 && ix < n) return ix;
+  switch (mode) {
+    case CIMX_MODE_REFLECT:
+      if (ix >= -n && ix < 2 * n) return ix < 0 ? -1 - ix : 2 * n - 1 - ix;
+      break;
+    case CIMX_MODE_MIRROR:
+      if (n == 1) return 0;
+      if (ix > -n && ix < 2 * n - 1) return ix < 0 ? -ix : 2 * n - 2 - ix;
+      break;
+    case CIMX_MODE_NEAREST:
+      return ix < 0 ? 0 : n - 1;
+    case CIMX_MODE_GRID_WRAP:
+      if (ix >= -n && ix < 2 * n) return ix < 0 ? ix + n : ix - n;
+      break;
+    default:
+      return -1;
+  }
+  return map_coord(ix, n, mode);
+}
+
 }  // namespace cimx

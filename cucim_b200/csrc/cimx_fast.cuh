@@ -453,8 +453,8 @@ template <class T>
 __device__ __forceinline__ float staged_value(const T* in, long long gy, long long gx,
                                               const SlabArgs& a, int my, int mx, float cy) {
   long long yy = gy, xx = gx;
-  if (gy < 0 || gy >= a.Y) yy = map_coord(gy, a.Y, my);
-  if (gx < 0 || gx >= a.X) xx = map_coord(gx, a.X, mx);
+  if (gy < 0 || gy >= a.Y) yy = map_coord_near(gy, a.Y, my);
+  if (gx < 0 || gx >= a.X) xx = map_coord_near(gx, a.X, mx);
   if (yy < 0) return cy;
   if (xx < 0) return 0.f;  // x-constant columns are replaced after the y pass
   return static_cast<float>(in[yy * a.X + xx]);
@@ -542,19 +542,53 @@ __global__ void __launch_bounds__(Geom<T, KB>::NT, Geom<T, KB>::MINB) k_slab(con
   if (G::F32 && TMA) {
     // the tile is already float: rewrite only the staged elements that lie
     // outside the array with their boundary-mode values
+    // (the same test for every thread of the CTA, so the barrier inside holds)
     if (!(rl == 0 && rr == G::RY && cl == 0 && cr == G::RX)) {
       float* rawf = reinterpret_cast<float*>(raw);
-      for (int r = warp; r < G::RY; r += G::NW) {
+      // Only the staged elements outside the array are visited, spread over
+      // every thread of the CTA.
+      // 1. rows inside the array: a column outside takes the value of the
+      //    column it maps to, read from the staged tile when that column is
+      //    staged (always, for overhangs shorter than the row), else from HBM;
+      //    x-constant columns hold 0 until the y pass replaces them
+      const int nleft = cl, nout = cl + (G::RX - cr);
+      const int n1 = (rr - rl) * nout;
+      for (int t = threadIdx.x; t < n1; t += G::NT) {
+        const int r = rl + t / nout, j = t % nout;
+        const int c = j < nleft ? j : cr + (j - nleft);
         float* row = rawf + r * G::BX + off;
-        if (r < rl || r >= rr) {
-          for (int c = lane; c < G::RX; c += 32)
-            row[c] = staged_value<T>(in, ys + r, xst + c, a, my, mx, cy);
-        } else {
-          for (int c = lane; c < cl; c += 32)
-            row[c] = staged_value<T>(in, ys + r, xst + c, a, my, mx, cy);
-          for (int c = cr + lane; c < G::RX; c += 32)
-            row[c] = staged_value<T>(in, ys + r, xst + c, a, my, mx, cy);
+        const long long xm = map_coord_near(xst + c, a.X, mx);
+        float v = 0.f;
+        if (xm >= 0) {
+          const long long sc = xm - xst;
+          if (sc >= cl && sc < cr) {
+            v = row[sc];
+          } else {
+            v = static_cast<float>(in[(ys + r) * a.X + xm]);
+          }
         }
+        row[c] = v;
+      }
+      __syncthreads();
+      // 2. rows outside the array: the fill value (constant mode), or a copy
+      //    of the (now complete) staged row they map to, else from HBM
+      const int nrow_out = G::RY - (rr - rl);
+      const int n2 = nrow_out * G::RX;
+      for (int t = threadIdx.x; t < n2; t += G::NT) {
+        const int q = t / G::RX, c = t % G::RX;
+        const int r = q < rl ? q : rr + (q - rl);
+        float* row = rawf + r * G::BX + off;
+        const long long ym = map_coord_near(ys + r, a.Y, my);
+        const long long sr = ym - ys;
+        float v;
+        if (ym < 0) {
+          v = cy;
+        } else if (sr >= rl && sr < rr) {
+          v = rawf[sr * G::BX + off + c];
+        } else {
+          v = staged_value<T>(in, ys + r, xst + c, a, my, mx, cy);
+        }
+        row[c] = v;
       }
     }
   } else {

@@ -36,7 +36,7 @@ __global__ void __launch_bounds__(256) k_minmax1d(const MinMaxArgs a) {
     double value = load_as<double>(a.in, idx, a.tin);
     for (int k = 0; k < a.size; ++k) {
       const long long c = l - a.anchor + k;
-      const long long m = (c >= 0 && c < a.L) ? c : map_coord(c, a.L, a.mode);
+      const long long m = (c >= 0 && c < a.L) ? c : map_coord_near(c, a.L, a.mode);
       const double v = m < 0 ? a.cval : load_as<double>(a.in, base + m * a.inner, a.tin);
       value = a.is_max ? fmax(v, value) : fmin(v, value);
     }

@@ -92,7 +92,7 @@ __device__ __forceinline__ void tap_loop(W (&acc)[P], const W* taps, int K, At a
 // Value of line coordinate c (boundary mode applied) of a float32 input.
 __device__ __forceinline__ float staged_f32(const float* line, long long stride, long long c,
                                             long long L, int mode, float cv) {
-  const long long m = (c >= 0 && c < L) ? c : map_coord(c, L, mode);
+  const long long m = (c >= 0 && c < L) ? c : map_coord_near(c, L, mode);
   return m < 0 ? cv : __ldg(line + m * stride);
 }
 
@@ -153,7 +153,7 @@ __global__ void __launch_bounds__(256) k_rows(GArgs a, TapBlock<W> tb) {
       }
     } else {
       for (int j = threadIdx.x; j < span; j += blockDim.x) {
-        const long long m = map_coord(x0 - a.anchor + j, a.L, a.mode);
+        const long long m = map_coord_near(x0 - a.anchor + j, a.L, a.mode);
         rb[j + (j >> 3)] = m < 0 ? cv : load_as<W>(a.in, rbase + m, a.tin);
       }
     }
@@ -235,7 +235,7 @@ __global__ void __launch_bounds__(256) k_cols(GArgs a, TapBlock<W> tb) {
     for (int j = threadIdx.y; j < span; j += kColTY) {
       W v = W(0);
       if (i < a.inner) {
-        const long long m = map_coord(l0 - a.anchor + j, a.L, a.mode);
+        const long long m = map_coord_near(l0 - a.anchor + j, a.L, a.mode);
         v = m < 0 ? cv : load_as<W>(a.in, (obase + m) * a.inner + i, a.tin);
       }
       buf[j * kColTI + threadIdx.x] = v;
@@ -272,7 +272,7 @@ __global__ void __launch_bounds__(256) k_direct(GArgs a) {
     for (int k = 0; k < a.K; ++k) {
       const W w = taps[k];
       if (SKIPZ && w == W(0)) continue;
-      const long long m = map_coord(l - a.anchor + k, a.L, a.mode);
+      const long long m = map_coord_near(l - a.anchor + k, a.L, a.mode);
       const W x = m < 0 ? cv : load_as<W>(a.in, (obase + m) * a.inner + i, a.tin);
       acc = fma(x, w, acc);
     }
