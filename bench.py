@@ -175,11 +175,14 @@ def step_ops(ndi, x, outs):
 # uniform filter: one launch of the volume kernel
 LAUNCHES_PER_STEP = 6
 
-# DRAM bytes per launch measured by ncu on a 64 x 1024 x 1024 stack
-TRAFFIC_64 = {"slab f32->f32 gaussian y,x K=17,17": 268.507136e6 + 227.813888e6,
-              "volume u16->f32 sobel K=3,3,3": 134.852352e6 + 211.893248e6}
-TRAFFIC_PROFILE = {"slab f32->f32 gaussian y,x K=17,17": "k_slab_f32_gaussian_yx_64x1024x1024.md",
-                   "volume u16->f32 sobel K=3,3,3": "k_vol_u16_f32_sobel_64x1024x1024.md"}
+# DRAM bytes per launch measured by ncu on a smaller stack: (bytes, slices of
+# that stack, profile file)
+TRAFFIC = {
+    "slab f32->f32 gaussian y,x K=17,17": (201.398272e6 + 162.961920e6, 48,
+                                           "k_slab_f32_gaussian_yx_48x1024x1024_and_2048x2048.md"),
+    "volume u16->f32 sobel K=3,3,3": (134.852352e6 + 211.893248e6, 64,
+                                      "k_vol_u16_f32_sobel_64x1024x1024.md"),
+}
 
 
 def reduce_step_time(ms, world, device, dist, torch):
@@ -617,12 +620,13 @@ def main():
         roof = {"bound": "hbm", "kernel": name, "achieved": kr["gbs"], "peak": hbm,
                 "unit": "GB/s", "frac": kr["gbs"] / hbm, "traffic": None,
                 "peak_source": "measured" if peaks else "fallback"}
-        if name in TRAFFIC_64 and args.shape is None:
-            # DRAM bytes of the same kernel captured by ncu on a 64-slice stack,
+        if name in TRAFFIC and args.shape is None:
+            # DRAM bytes of the same kernel captured by ncu on a smaller stack,
             # scaled to the 512-slice launch (traffic grows with the slices)
-            roof["traffic"] = TRAFFIC_64[name] * SHAPE[0] / 64
-            roof["traffic_source"] = ("ncu dram__bytes_read + dram__bytes_write of the same kernel on "
-                                      "64 x 1024 x 1024, x 512/64 (profiles/" + TRAFFIC_PROFILE[name] + ")")
+            tb, slices, prof = TRAFFIC[name]
+            roof["traffic"] = tb * SHAPE[0] / slices
+            roof["traffic_source"] = (f"ncu dram__bytes_read + dram__bytes_write of the same kernel on "
+                                      f"{slices} x 1024 x 1024, x 512/{slices} (profiles/{prof})")
         cpu = None
         if not args.no_cpu:
             cpu = cpu_baseline(res["x"].numpy())
