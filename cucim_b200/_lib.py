@@ -103,6 +103,8 @@ _sigs = {
         [_A, _A, _P(CimxPass), ctypes.c_int, ctypes.c_int, ctypes.c_void_p], ctypes.c_int,
     ),
     "cimx_combine": ([_A, _A, ctypes.c_int, ctypes.c_void_p], ctypes.c_int),
+    "cimx_square_accumulate": ([_A, _A, ctypes.c_int, ctypes.c_void_p], ctypes.c_int),
+    "cimx_sqrt": ([_A, ctypes.c_void_p], ctypes.c_int),
     "cimx_unsharp": (
         [_A, _A, _A, ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_double,
          ctypes.c_void_p],

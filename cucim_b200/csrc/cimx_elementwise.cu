@@ -485,6 +485,30 @@ int cimx_gradient_magnitude(const CimxArray* in, const CimxArray* out, const Cim
   return rc;
 }
 
+int cimx_square_accumulate(const CimxArray* acc, const CimxArray* term, int first,
+                           void* stream) {
+  if (!acc || !term) return fail(CIMX_E_INVALID, "bad square-accumulate arguments");
+  if (acc->dtype != DT_F32 && acc->dtype != DT_F64)
+    return fail(CIMX_E_DTYPE, "square-accumulate: float32 or float64");
+  if (term->dtype != acc->dtype) return fail(CIMX_E_DTYPE, "square-accumulate: dtypes differ");
+  if (!same_shape(acc, term)) return fail(CIMX_E_INVALID, "square-accumulate: shapes differ");
+  if (!contiguous(acc) || !contiguous(term))
+    return fail(CIMX_E_LAYOUT, "square-accumulate: arrays must be C-contiguous");
+  const int64_t n = numel(acc);
+  if (n == 0) return CIMX_OK;
+  return launch_square_accumulate(acc->data, term->data, acc->dtype, n, first != 0,
+                                  static_cast<cudaStream_t>(stream));
+}
+
+int cimx_sqrt(const CimxArray* a, void* stream) {
+  if (!a) return fail(CIMX_E_INVALID, "bad sqrt arguments");
+  if (a->dtype != DT_F32 && a->dtype != DT_F64) return fail(CIMX_E_DTYPE, "sqrt: float32 or float64");
+  if (!contiguous(a)) return fail(CIMX_E_LAYOUT, "sqrt: array must be C-contiguous");
+  const int64_t n = numel(a);
+  if (n == 0) return CIMX_OK;
+  return launch_sqrt_inplace(a->data, a->dtype, n, static_cast<cudaStream_t>(stream));
+}
+
 int cimx_combine(const CimxArray* acc, const CimxArray* term, int op, void* stream) {
   if (!acc || !term || (op != CIMX_COMBINE_ADD && op != CIMX_COMBINE_SUBTRACT))
     return fail(CIMX_E_INVALID, "bad combine arguments");

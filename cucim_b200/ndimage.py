@@ -549,7 +549,9 @@ def maximum_filter1d(input, size, axis=-1, output=None, mode="reflect", cval=0.0
 
 def generic_gradient_magnitude(input, derivative, output=None, mode="reflect", cval=0.0,
                                extra_arguments=(), extra_keywords=None, *, axes=None):
-    """FLT:1012-1097 with a user-supplied derivative callable."""
+    """FLT:1012-1097 with a user-supplied derivative callable: the squares,
+    sums and square root run in libcimx, each operation rounded on its own
+    as CuPy's in-place operators round it."""
     if extra_keywords is None:
         extra_keywords = {}
     x = _arrays.as_tensor(input)
@@ -560,24 +562,33 @@ def generic_gradient_magnitude(input, derivative, output=None, mode="reflect", c
     if ndim == 0:
         slot.work.copy_(x)
         return slot.result()
-    if slot.dtype.kind != "f":
-        raise NotImplementedError("generic_gradient_magnitude supports float outputs only")
-    res = _arrays.as_tensor(derivative(input, axes[0], slot.work, modes[0], cval,
-                                       *extra_arguments, **extra_keywords))
+    if slot.dtype.kind != "f" or slot.dtype.itemsize < 4:
+        raise NotImplementedError(
+            "generic_gradient_magnitude supports float32 / float64 outputs only")
+
+    def into(res, dst):
+        r = _arrays.as_tensor(res)
+        if r.data_ptr() != dst.data_ptr():
+            dst.copy_(r)
+
+    def square_acc(acc, term, first):
+        a_acc, a_t = _arrays.to_cimx(acc), _arrays.to_cimx(term)
+        rc = _lib.lib.cimx_square_accumulate(ctypes.byref(a_acc), ctypes.byref(a_t),
+                                             1 if first else 0, _arrays.stream_of(acc))
+        _lib.check(rc, "gradient magnitude")
+
     acc = slot.work
-    if res.data_ptr() != acc.data_ptr():
-        acc.copy_(res)
-    acc.mul_(acc)
+    into(derivative(input, axes[0], acc, modes[0], cval, *extra_arguments, **extra_keywords),
+         acc)
+    square_acc(acc, acc, True)
     if len(axes) > 1:
         tmp = torch.empty_like(acc)
         for i in range(1, len(axes)):
-            r = _arrays.as_tensor(derivative(input, axes[i], tmp, modes[i], cval,
-                                             *extra_arguments, **extra_keywords))
-            if r.data_ptr() != tmp.data_ptr():
-                tmp.copy_(r)
-            tmp.mul_(tmp)
-            acc.add_(tmp)
-    acc.sqrt_()
+            into(derivative(input, axes[i], tmp, modes[i], cval, *extra_arguments,
+                            **extra_keywords), tmp)
+            square_acc(acc, tmp, False)
+    a_acc = _arrays.to_cimx(acc)
+    _lib.check(_lib.lib.cimx_sqrt(ctypes.byref(a_acc), _arrays.stream_of(acc)), "sqrt")
     return slot.result()
 
 

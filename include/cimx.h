@@ -180,6 +180,15 @@ CIMX_API int cimx_gradient_magnitude(const CimxArray* in, const CimxArray* out,
 CIMX_API int cimx_laplace(const CimxArray* in, const CimxArray* out, const CimxPass* passes,
                           int naxes, int passes_per_axis, void* stream);
 
+/* acc = term * term (first != 0) or acc + term * term, each operation rounded
+ * on its own; and acc = sqrt(acc) in place. float32 or float64, equal
+ * dtypes and shapes, C-contiguous: the `output *= output; tmp *= tmp;
+ * output += tmp; cupy.sqrt(output, output)` of generic_gradient_magnitude
+ * with a user derivative (_vendored/_ndimage_filters.py:1012-1097). */
+CIMX_API int cimx_square_accumulate(const CimxArray* acc, const CimxArray* term, int first,
+                                    void* stream);
+CIMX_API int cimx_sqrt(const CimxArray* a, void* stream);
+
 /* acc = acc + term (op CIMX_COMBINE_ADD) or acc - term (CIMX_COMBINE_SUBTRACT)
  * in acc's dtype: integers wrap, floats round to nearest. Both arrays have
  * the same dtype and shape and are C-contiguous. The in-place `output += tmp`

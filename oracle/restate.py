@@ -521,6 +521,31 @@ def maximum_filter1d(input, size, axis=-1, output=None, mode="reflect", cval=0.0
     return _min_or_max_1d(input, size, axis, output, mode, cval, origin, True)
 
 
+def generic_gradient_magnitude(input, derivative, output=None, mode="reflect", cval=0.0,
+                               extra_arguments=(), extra_keywords=None, *, axes=None):
+    """FLT:1012-1097: output = d0, output *= output, then tmp = d_i,
+    tmp *= tmp, output += tmp for the other axes, sqrt in place (numpy
+    operations in the output dtype)."""
+    input = np.asarray(input)
+    if extra_keywords is None:
+        extra_keywords = {}
+    axes = check_axes(axes, input.ndim)
+    modes = fix_sequence_arg(mode, len(axes), "mode", check_mode)
+    out = get_output(output, input)
+    out[...] = derivative(input, axes[0], out, modes[0], cval, *extra_arguments,
+                          **extra_keywords)
+    np.multiply(out, out, out=out)
+    if len(axes) > 1:
+        tmp = np.empty_like(out)
+        for i in range(1, len(axes)):
+            tmp[...] = derivative(input, axes[i], tmp, modes[i], cval, *extra_arguments,
+                                  **extra_keywords)
+            np.multiply(tmp, tmp, out=tmp)
+            np.add(out, tmp, out=out)
+    np.sqrt(out, out=out)
+    return out
+
+
 def generic_laplace(input, derivative2, output=None, mode="reflect", cval=0.0,
                     extra_arguments=(), extra_keywords=None, *, axes=None):
     """FLT:806-890: derivative2 along the first axis into the output, every

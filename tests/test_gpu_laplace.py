@@ -172,3 +172,18 @@ def test_min_max_filter1d_nan_outputs_and_errors(ndi):
         ndi.minimum_filter1d(xd, 0)
     with pytest.raises(ValueError):
         ndi.minimum_filter1d(xd, 3, origin=2)
+
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_generic_gradient_magnitude_user_callable(ndi, dtype):
+    # FLT:1012-1097 with a user derivative: squares, sums and sqrt in libcimx
+    x = _data((14, 30, 36), dtype)
+    got = host(ndi.generic_gradient_magnitude(dev(x), ndi.sobel, mode="nearest"))
+    exp = R.generic_gradient_magnitude(x, R.sobel, mode="nearest")
+    np.testing.assert_array_equal(got, exp)
+    got = host(ndi.generic_gradient_magnitude(dev(x), ndi.prewitt, axes=(0, 2),
+                                              mode=("mirror", "constant"), cval=2.0))
+    exp = R.generic_gradient_magnitude(x, R.prewitt, axes=(0, 2), mode=("mirror", "constant"),
+                                       cval=2.0)
+    np.testing.assert_array_equal(got, exp)
