@@ -39,6 +39,7 @@ F_SKIP_ZERO_TAPS = 1 << 3
 L_NO_FUSION = 1 << 0
 L_TENSOR_BF16X3 = 1 << 1
 L_TENSOR_TF32X3 = 1 << 2
+L_TENSOR_ALL_LINES = 1 << 3
 
 E_INVALID, E_DTYPE, E_CUDA, E_NOMEM, E_LAYOUT, E_TIMEOUT = -1, -2, -3, -4, -5, -6
 

@@ -246,8 +246,28 @@ int cimx_separable(const CimxArray* in, const CimxArray* out, const CimxPass* pa
 
   const bool tf32x3 = (lib_flags & CIMX_L_TENSOR_TF32X3) != 0;
   const bool tensor = tf32x3 || (lib_flags & CIMX_L_TENSOR_BF16X3) != 0;
+  // Tensor-core passes where they measured faster than the plain kernels: on
+  // a B200, 1.2-2.3x for 23-143 taps along 8192-sample lines, slower or even
+  // for every length along 256-sample lines (the band's halo and the strip
+  // set-up dominate short lines). CIMX_L_TENSOR_ALL_LINES lifts the limit.
+  constexpr int64_t kTensorMinLine = 2048;
+  const bool all_lines = (lib_flags & CIMX_L_TENSOR_ALL_LINES) != 0;
+  auto tensor_kind = [&](const PassDesc& d) {
+    if (!tensor || d.K < 16 || (!all_lines && d.L < kTensorMinLine)) return 0;
+    if (tf32x3) return tcs_supports(d) ? 1 : 0;
+    return tc_supports(d) ? 2 : 0;
+  };
+  bool any_tensor = false;
+  for (int i = 0; i < npasses; ++i) {
+    PassDesc d = ds[i];  // the dtypes each pass will see
+    d.in = in->data;
+    d.out = out->data;
+    d.tin = i == 0 ? in->dtype : out->dtype;
+    d.tout = out->dtype;
+    any_tensor = any_tensor || tensor_kind(d) != 0;
+  }
   // fused kernels take whole runs of passes in one launch
-  if (!tensor && !(lib_flags & CIMX_L_NO_FUSION)) {
+  if (!any_tensor && !(lib_flags & CIMX_L_NO_FUSION)) {
     rc = try_fused(in, out, ds.data(), npasses, st);
     if (rc != CIMX_FUSED_DECLINED) return rc;
     rc = CIMX_OK;
@@ -269,9 +289,10 @@ int cimx_separable(const CimxArray* in, const CimxArray* out, const CimxPass* pa
     ds[i].tin = tsrc;
     ds[i].out = dst;
     ds[i].tout = out->dtype;
-    if (tf32x3 && ds[i].K >= 16 && tcs_supports(ds[i]))
+    const int kind = tensor_kind(ds[i]);
+    if (kind == 1)
       rc = launch_tcs_pass(ds[i], st);
-    else if (tensor && !tf32x3 && ds[i].K >= 16 && tc_supports(ds[i]))
+    else if (kind == 2)
       rc = launch_tc_pass(ds[i], st);
     else
       rc = launch_generic_pass(ds[i], st);

@@ -88,8 +88,9 @@ def _build_passes(in_dtype, out_dtype, ndim, specs, cval, algorithm):
 
 # algorithm="tensor" and "tensor_bf16x3": additions of this library (cuCIM
 # accepts only "shared_memory", "elementwise" and None). float32 -> float32
-# passes with at least 16 taps run on the tensor cores as banded-Toeplitz
-# products with float32 accumulation: "tensor" splits operands into tf32
+# passes with at least 16 taps along lines of at least 2048 samples (where
+# they measured faster; see tensor_cores_everywhere) run on the tensor cores
+# as banded-Toeplitz products with float32 accumulation: "tensor" splits operands into tf32
 # hi + lo (TF32x3, max relative error near 1e-6), "tensor_bf16x3" into
 # bfloat16 hi + lo (BF16x3, near 1e-5). Results are close to, not
 # bit-identical with, the float32 chain. Other passes run as usual.
@@ -133,6 +134,22 @@ def _hashable(obj):
 # keyed by everything they depend on: repeated calls with the same filter
 # skip the tap arithmetic and the struct building.
 _PASS_CACHE = {}
+
+
+@contextlib.contextmanager
+def tensor_cores_everywhere():
+    """Within this block algorithm="tensor" / "tensor_bf16x3" runs every
+    eligible pass on the tensor cores, whatever its line length. By default
+    only passes along lines of at least 2048 samples do (on shorter lines the
+    plain kernels measured faster). A testing and measurement aid, not
+    thread-safe."""
+    global _EXTRA_LIB_FLAGS
+    old = _EXTRA_LIB_FLAGS
+    _EXTRA_LIB_FLAGS = old | _lib.L_TENSOR_ALL_LINES
+    try:
+        yield
+    finally:
+        _EXTRA_LIB_FLAGS = old
 
 
 def _run(input, specs, output, cval, algorithm=None, cache_key=None):

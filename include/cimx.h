@@ -70,7 +70,9 @@ enum {
 /* Library-level flags for multi-pass calls. */
 enum {
   CIMX_L_NO_FUSION = 1 << 0,    /* force one launch per pass (ping-pong through scratch) */
-  CIMX_L_TENSOR_BF16X3 = 1 << 1,/* run float32 -> float32 passes with at least 16 taps on the
+  CIMX_L_TENSOR_BF16X3 = 1 << 1,/* run float32 -> float32 passes with at least 16 taps along
+                                   lines of at least 2048 samples (where they measured faster
+                                   than the plain kernels) on the
                                    tensor cores: banded-Toeplitz products of bfloat16 hi/lo
                                    splits, float32 accumulation (not bit-identical to the
                                    float32 chain; an addition of this library) */
@@ -78,6 +80,8 @@ enum {
                                    streaming TMA-fed kernel: about ten times more accurate
                                    than BF16X3 (a relative error per product near 2^-21) and
                                    faster; takes precedence when both bits are set */
+  CIMX_L_TENSOR_ALL_LINES = 1 << 3,/* with a tensor bit: every eligible pass on the tensor
+                                   cores whatever its line length (testing, measurement) */
 };
 
 /* One 1-D correlation pass of a separable filter. */

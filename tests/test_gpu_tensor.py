@@ -35,6 +35,15 @@ def ndi(cuda):
     return ndimage
 
 
+@pytest.fixture(autouse=True)
+def _tensor_cores_on_short_lines(ndi):
+    # most shapes here have lines shorter than the 2048 samples from which
+    # algorithm="tensor" uses the tensor cores by default: force them, so
+    # that these tests exercise the tensor-core kernels
+    with ndi.tensor_cores_everywhere():
+        yield
+
+
 def _check(got, ref, algo, passes=None):
     err = np.abs(got.astype(np.float64) - ref)
     scale = max(np.abs(ref).max(), 1e-30)
