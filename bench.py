@@ -525,6 +525,14 @@ def run_plain2d(torch, dev, n_img=16, reps=5, hbm_gbs=None):
                             "of each call) and one skimage.filters.gaussian call per image"}
     if hbm_gbs:
         res["frac_of_hbm"] = gbs / hbm_gbs
+    # 33 taps on each of two axes: 2 * 2 * 33 useful flops per pixel, which
+    # at the nominal FP32 rate (148 SMs x 128 FMA lanes x 2 x 1965 MHz) take
+    # longer than the 8 bytes per pixel at the measured copy bandwidth
+    tflops = 2 * 2 * 33 * base.numel() / (ms_kernel * 1e-3) / 1e12
+    fp32_nominal = 148 * 128 * 2 * 1.965e9 / 1e12
+    res["fp32_tflops"] = tflops
+    res["fp32_nominal_tflops"] = fp32_nominal
+    res["frac_of_fp32_nominal"] = tflops / fp32_nominal
     return res
 
 
