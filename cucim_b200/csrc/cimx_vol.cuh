@@ -371,9 +371,12 @@ int launch_vol_km(const VolArgs& v, cudaStream_t st) {
   a.tiles_x = static_cast<int>((v.X + kTX - 1) / kTX);
   const long long tiles = (long long)a.tiles_x * ((v.Y + TY - 1) / TY);
   // z chunk: long enough that the K - 1 extra slices stay a small share,
-  // short enough for a few waves of CTAs (one per SM)
+  // short enough for a few waves of CTAs (one per SM). Measured on the
+  // 512 x 1024 x 1024 uint16 stack: 3 taps ran 2.3 % faster with 32-slice
+  // chunks (12 waves) than with 64; 5 taps showed no such gain.
+  const long long waves = K == 3 ? 12 : 6;
   int zc = 128;
-  while (zc > 16 && tiles * ((v.Z + zc - 1) / zc) * v.B < 148LL * 6) zc /= 2;
+  while (zc > 16 && tiles * ((v.Z + zc - 1) / zc) * v.B < 148LL * waves) zc /= 2;
   a.zchunk = zc;
   const long long nzc = (v.Z + zc - 1) / zc;
   if (tiles > 0x7fffffffLL || nzc > 65535) return CIMX_FUSED_DECLINED;
