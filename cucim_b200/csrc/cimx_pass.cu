@@ -316,9 +316,10 @@ __device__ __forceinline__ void tap_loop_pairs(u64 (&acc)[P], const u64* taps, i
 // one f32x2 FMA per tap and output pair, and a tile is 32 columns x 128
 // outputs (half the halo share of k_cols' 64-output tiles). Four CTAs per
 // SM: with three (80 registers) the staging loads of short-tap passes had
-// too few warps in flight and ran 10 % slower than k_cols; with four it
-// matches k_cols up to 57 taps and is 23 % faster at 143 (256^3 float32,
-// axis 0).
+// too few warps in flight. The boundary map runs once per staged row (a
+// table of row offsets in shared memory) rather than per element, which
+// took a fifth of the time off every pass. 256^3 float32, axis 0: 70, 95
+// and 152 us at 23, 57 and 143 taps, against 89, 129 and 242 us for k_cols.
 template <bool SKIPZ>
 __global__ void __launch_bounds__(256, 4) k_cols_pairs(GArgs a, TapBlock<float> tb) {
   extern __shared__ __align__(16) unsigned char sm_raw[];
@@ -333,6 +334,9 @@ __global__ void __launch_bounds__(256, 4) k_cols_pairs(GArgs a, TapBlock<float> 
   }
   float* buf = reinterpret_cast<float*>(taps + a.K8);  // span rows x 32 columns
   const int span = kCol2TL + a.K8 + P;
+  // element offset of each staged row's mapped line coordinate, -1 for the
+  // fill value: the boundary map runs once per row, not per element
+  long long* rowoff = reinterpret_cast<long long*>(buf + (size_t)span * 32);
 
   long long bid = blockIdx.x;
   const long long it = bid % a.tiles_a;
@@ -342,23 +346,30 @@ __global__ void __launch_bounds__(256, 4) k_cols_pairs(GArgs a, TapBlock<float> 
   const long long l0 = lt * kCol2TL;
   const float cv = fill_value<float>(a.cval, a.cval_as_input, a.tin);
   const long long obase = o * a.L;
+  const long long c0 = l0 - a.anchor;
+  for (int j = tid; j < span; j += 256) {
+    const long long cj = c0 + j;
+    const long long m = (cj >= 0 && cj < a.L) ? cj : map_coord_near(cj, a.L, a.mode);
+    rowoff[j] = m < 0 ? -1 : m * a.inner;
+  }
+  __syncthreads();
   {
     // staging: thread (c, r) loads column c of rows r, r + 8, ..., eight
     // loads in flight before the stores
     const int c = tid & 31, r = tid >> 5;
     const long long ic = it * 32 + c;
     const float* col = static_cast<const float*>(a.in) + obase * a.inner + ic;
-    const long long c0 = l0 - a.anchor;
-    const bool interior = c0 >= 0 && c0 + span <= a.L;
+    const bool cin = ic < a.inner;
     for (int jb = r; jb < span; jb += 64) {
       float v[8];
 #pragma unroll
       for (int q = 0; q < 8; ++q) {
         const int j = jb + q * 8;
         v[q] = 0.f;
-        if (j < span && ic < a.inner)
-          v[q] = interior ? __ldg(col + (c0 + j) * a.inner)
-                          : staged_f32(col, a.inner, c0 + j, a.L, a.mode, cv);
+        if (j < span && cin) {
+          const long long off = rowoff[j];
+          v[q] = off < 0 ? cv : __ldg(col + off);
+        }
       }
 #pragma unroll
       for (int q = 0; q < 8; ++q) {
@@ -444,7 +455,8 @@ int launch_t(GArgs a, const TapBlock<W>& tb, bool direct, cudaStream_t st) {
   } else {
     if constexpr (std::is_same<W, float>::value) {
       // float32 input along lines longer than one k_cols tile: column pairs
-      const size_t smem2 = 8 * (size_t)a.K8 + sizeof(float) * (size_t)(kCol2TL + a.K8 + P) * 32;
+      const size_t span2 = (size_t)(kCol2TL + a.K8 + P);
+      const size_t smem2 = 8 * (size_t)a.K8 + sizeof(float) * span2 * 32 + 8 * span2;
       if (a.tin == DT_F32 && a.inner >= 2 && a.L > kColTL && smem2 <= (size_t)kMaxSmem) {
         a.tiles_a = (a.inner + 31) / 32;
         a.tiles_b = (a.L + kCol2TL - 1) / kCol2TL;
