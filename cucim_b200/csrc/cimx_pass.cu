@@ -188,6 +188,9 @@ __global__ void __launch_bounds__(256) k_cols(GArgs a, TapBlock<W> tb) {
   load_taps(taps, a, tb, tid, kColTI * kColTY);
   W* buf = taps + a.K8;
   const int span = kColTL + a.K8 + P;
+  // element index of each staged row's mapped line coordinate (column 0),
+  // -1 for the fill value: the boundary map runs once per row
+  long long* rowoff = reinterpret_cast<long long*>(buf + (size_t)span * kColTI);
 
   long long bid = blockIdx.x;
   const long long it = bid % a.tiles_a;
@@ -199,7 +202,16 @@ __global__ void __launch_bounds__(256) k_cols(GArgs a, TapBlock<W> tb) {
   const W cv = fill_value<W>(a.cval, a.cval_as_input, a.tin);
   const long long obase = o * a.L;
   const bool interior = l0 - a.anchor >= 0 && l0 - a.anchor + span <= a.L;
-  if (sizeof(W) == 4 && a.tin == DT_F32 && interior) {
+  const bool walk = sizeof(W) == 4 && a.tin == DT_F32 && interior;
+  if (!walk) {  // the same for every thread of the CTA
+    for (int j = tid; j < span; j += kColTI * kColTY) {
+      const long long cj = l0 - a.anchor + j;
+      const long long m = map_coord_near(cj, a.L, a.mode);
+      rowoff[j] = m < 0 ? -1 : (obase + m) * a.inner;
+    }
+    __syncthreads();
+  }
+  if (walk) {
     // float32 input, span inside the line: a pointer walk, eight loads in flight
     const long long stride = a.inner;
     const float* col = static_cast<const float*>(a.in) + (obase + l0 - a.anchor) * stride + i;
@@ -218,15 +230,17 @@ __global__ void __launch_bounds__(256) k_cols(GArgs a, TapBlock<W> tb) {
     }
   } else if (sizeof(W) == 4 && a.tin == DT_F32) {
     // float32 input: eight loads in flight per thread before the stores
-    const float* col = static_cast<const float*>(a.in) + obase * a.inner + i;
+    const float* col = static_cast<const float*>(a.in) + i;
     for (int jb = threadIdx.y; jb < span; jb += 8 * kColTY) {
       float v[8];
 #pragma unroll
       for (int q = 0; q < 8; ++q) {
         const int j = jb + q * kColTY;
-        v[q] = (j < span && i < a.inner)
-                   ? staged_f32(col, a.inner, l0 - a.anchor + j, a.L, a.mode, (float)cv)
-                   : 0.f;
+        v[q] = 0.f;
+        if (j < span && i < a.inner) {
+          const long long off = rowoff[j];
+          v[q] = off < 0 ? (float)cv : __ldg(col + off);
+        }
       }
 #pragma unroll
       for (int q = 0; q < 8; ++q) {
@@ -238,8 +252,8 @@ __global__ void __launch_bounds__(256) k_cols(GArgs a, TapBlock<W> tb) {
     for (int j = threadIdx.y; j < span; j += kColTY) {
       W v = W(0);
       if (i < a.inner) {
-        const long long m = map_coord_near(l0 - a.anchor + j, a.L, a.mode);
-        v = m < 0 ? cv : load_as<W>(a.in, (obase + m) * a.inner + i, a.tin);
+        const long long off = rowoff[j];
+        v = off < 0 ? cv : load_as<W>(a.in, off + i, a.tin);
       }
       buf[j * kColTI + threadIdx.x] = v;
     }
@@ -465,7 +479,8 @@ int launch_t(GArgs a, const TapBlock<W>& tb, bool direct, cudaStream_t st) {
         return cuda_fail(cudaGetLastError(), "generic pass launch");
       }
     }
-    const size_t smem = sizeof(W) * ((size_t)a.K8 + (size_t)(kColTL + a.K8 + P) * kColTI);
+    const size_t smem = sizeof(W) * ((size_t)a.K8 + (size_t)(kColTL + a.K8 + P) * kColTI) +
+                        8 * (size_t)(kColTL + a.K8 + P);
     a.tiles_a = (a.inner + kColTI - 1) / kColTI;
     a.tiles_b = (a.L + kColTL - 1) / kColTL;
     const long long blocks = a.tiles_a * a.tiles_b * a.outer;
@@ -509,7 +524,8 @@ int launch_w(const PassDesc& d, cudaStream_t st) {
   std::fill(std::begin(tb.w), std::end(tb.w), W(0));
   const bool fits_param = K * sizeof(W) <= sizeof(tb.w);
   const size_t smem_rows = sizeof(W) * ((size_t)a.K8 + (size_t)(2048 + a.K8 + P) * 9 / 8 + 2);
-  const size_t smem_cols = sizeof(W) * ((size_t)a.K8 + (size_t)(kColTL + a.K8 + P) * kColTI);
+  const size_t smem_cols = sizeof(W) * ((size_t)a.K8 + (size_t)(kColTL + a.K8 + P) * kColTI) +
+                           8 * (size_t)(kColTL + a.K8 + P);
   const bool direct = (a.inner == 1 ? smem_rows : smem_cols) > (size_t)kMaxSmem;
   void* gt = nullptr;
   const size_t gbytes = sizeof(W) * std::max(K, 1);
