@@ -113,6 +113,10 @@ __global__ void __launch_bounds__(256) k_rows(GArgs a, TapBlock<W> tb) {
   const int span = seg + a.K8 + P;
   const int pspan = span + (span >> 3) + 1;
   W* rb = taps + a.K8 + threadIdx.y * pspan;
+  // mapped line coordinate of each staged column (-1: the fill value), shared
+  // by the rows of the CTA: the boundary map runs once per column
+  long long* colmap = reinterpret_cast<long long*>(
+      sm_raw + ((sizeof(W) * ((size_t)a.K8 + (size_t)blockDim.y * pspan) + 7) & ~(size_t)7));
 
   const long long sg = blockIdx.x % a.tiles_b;
   const long long rg = blockIdx.x / a.tiles_b;
@@ -120,9 +124,14 @@ __global__ void __launch_bounds__(256) k_rows(GArgs a, TapBlock<W> tb) {
   const long long x0 = sg * seg;
   const W cv = fill_value<W>(a.cval, a.cval_as_input, a.tin);
   const long long rbase = row * a.L;
+  const bool interior = x0 - a.anchor >= 0 && x0 - a.anchor + span <= a.L;
+  const bool walk = sizeof(W) == 4 && a.tin == DT_F32 && interior;
+  if (!walk) {  // the same for every thread of the CTA
+    for (int j = tid; j < span; j += nthr) colmap[j] = map_coord_near(x0 - a.anchor + j, a.L, a.mode);
+    __syncthreads();
+  }
   if (row < a.outer) {
-    const bool interior = x0 - a.anchor >= 0 && x0 - a.anchor + span <= a.L;
-    if (sizeof(W) == 4 && a.tin == DT_F32 && interior) {
+    if (walk) {
       // float32 input, span inside the row: plain loads, eight in flight
       const float* line = static_cast<const float*>(a.in) + rbase + (x0 - a.anchor);
       for (int jb = threadIdx.x; jb < span; jb += 8 * blockDim.x) {
@@ -146,7 +155,11 @@ __global__ void __launch_bounds__(256) k_rows(GArgs a, TapBlock<W> tb) {
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
           const int j = jb + q * blockDim.x;
-          v[q] = j < span ? staged_f32(line, 1, x0 - a.anchor + j, a.L, a.mode, (float)cv) : 0.f;
+          v[q] = 0.f;
+          if (j < span) {
+            const long long m = colmap[j];
+            v[q] = m < 0 ? (float)cv : __ldg(line + m);
+          }
         }
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
@@ -156,7 +169,7 @@ __global__ void __launch_bounds__(256) k_rows(GArgs a, TapBlock<W> tb) {
       }
     } else {
       for (int j = threadIdx.x; j < span; j += blockDim.x) {
-        const long long m = map_coord_near(x0 - a.anchor + j, a.L, a.mode);
+        const long long m = colmap[j];
         rb[j + (j >> 3)] = m < 0 ? cv : load_as<W>(a.in, rbase + m, a.tin);
       }
     }
@@ -437,6 +450,24 @@ __global__ void __launch_bounds__(256) k_direct(GArgs a) {
   }
 }
 
+// Row kernel geometry for lines of L samples: threads per segment, rows per
+// CTA and the dynamic shared memory (taps, padded row buffers, column map).
+struct RowGeom {
+  int seg_threads, ry, seg;
+  size_t smem;
+};
+inline RowGeom row_geom(long long L, int K8, size_t wsize) {
+  RowGeom g;
+  g.seg_threads = 256;
+  while (g.seg_threads > 32 && (long long)(g.seg_threads / 2) * P >= L) g.seg_threads /= 2;
+  g.ry = 256 / g.seg_threads;
+  g.seg = g.seg_threads * P;
+  const int span = g.seg + K8 + P;
+  const int pspan = span + (span >> 3) + 1;
+  g.smem = ((wsize * ((size_t)K8 + (size_t)g.ry * pspan) + 7) & ~(size_t)7) + 8 * (size_t)span;
+  return g;
+}
+
 template <class Kern>
 void allow_big_smem(Kern k) {
   cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem);
@@ -456,16 +487,10 @@ int launch_t(GArgs a, const TapBlock<W>& tb, bool direct, cudaStream_t st) {
     const long long blocks = std::min<long long>((total + 255) / 256, 148LL * 64);
     k_direct<W, SKIPZ><<<(unsigned)blocks, 256, 0, st>>>(a);
   } else if (a.inner == 1) {
-    int seg_threads = 256;
-    while (seg_threads > 32 && (long long)(seg_threads / 2) * P >= a.L) seg_threads /= 2;
-    const int ry = 256 / seg_threads;
-    const int seg = seg_threads * P;
-    const int span = seg + a.K8 + P;
-    const int pspan = span + (span >> 3) + 1;
-    const size_t smem = sizeof(W) * ((size_t)a.K8 + (size_t)ry * pspan);
-    a.tiles_b = (a.L + seg - 1) / seg;
-    const long long blocks = ((a.outer + ry - 1) / ry) * a.tiles_b;
-    k_rows<W, SKIPZ><<<(unsigned)blocks, dim3(seg_threads, ry), smem, st>>>(a, tb);
+    const RowGeom g = row_geom(a.L, a.K8, sizeof(W));
+    a.tiles_b = (a.L + g.seg - 1) / g.seg;
+    const long long blocks = ((a.outer + g.ry - 1) / g.ry) * a.tiles_b;
+    k_rows<W, SKIPZ><<<(unsigned)blocks, dim3(g.seg_threads, g.ry), g.smem, st>>>(a, tb);
   } else {
     if constexpr (std::is_same<W, float>::value) {
       // float32 input along lines longer than one k_cols tile: column pairs
@@ -523,7 +548,7 @@ int launch_w(const PassDesc& d, cudaStream_t st) {
   TapBlock<W> tb;
   std::fill(std::begin(tb.w), std::end(tb.w), W(0));
   const bool fits_param = K * sizeof(W) <= sizeof(tb.w);
-  const size_t smem_rows = sizeof(W) * ((size_t)a.K8 + (size_t)(2048 + a.K8 + P) * 9 / 8 + 2);
+  const size_t smem_rows = row_geom(a.L, a.K8, sizeof(W)).smem;
   const size_t smem_cols = sizeof(W) * ((size_t)a.K8 + (size_t)(kColTL + a.K8 + P) * kColTI) +
                            8 * (size_t)(kColTL + a.K8 + P);
   const bool direct = (a.inner == 1 ? smem_rows : smem_cols) > (size_t)kMaxSmem;

@@ -26,6 +26,7 @@
  */
 #include <math.h>
 #include <stdint.h>
+#include <stdlib.h>
 #include <string.h>
 
 enum { M_REFLECT = 0, M_MIRROR = 1, M_NEAREST = 2, M_GRID_WRAP = 3, M_CONSTANT = 4 };
@@ -240,9 +241,10 @@ void oracle_correlate1d(const void* in, int tin, void* out, int tout, int64_t ou
                         int64_t L, int64_t inner, const double* taps, int K, int anchor,
                         int mode, double cval_w, int w64, int skip_zero, int threads) {
   const int64_t nlines = outer * inner;
-  float wf[4096];
-  int Kc = K < 4096 ? K : 4096;
-  for (int k = 0; k < Kc; ++k) wf[k] = (float)taps[k];
+  /* float32 copies of the taps, any K (heap: tap counts reach the thousands) */
+  float* wf = (float*)malloc(sizeof(float) * (size_t)(K > 0 ? K : 1));
+  if (!wf) return;
+  for (int k = 0; k < K; ++k) wf[k] = (float)taps[k];
 #if defined(_OPENMP)
 #pragma omp parallel for schedule(static) num_threads(threads > 0 ? threads : 1)
 #else
@@ -283,6 +285,7 @@ void oracle_correlate1d(const void* in, int tin, void* out, int tout, int64_t ou
       }
     }
   }
+  free(wf);
 }
 
 /* Elementwise cast of a W-typed array (float32 when w64 == 0) into dtype dt

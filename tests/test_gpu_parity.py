@@ -130,6 +130,21 @@ def test_long_kernels(ndi, K, shape):
         np.testing.assert_array_equal(got, exp)
 
 
+@pytest.mark.parametrize("dtype", [np.float32, np.uint16])
+def test_very_long_kernel_short_rows(ndi, dtype):
+    """8001 taps on 100-sample rows: the row kernel packs 8 rows per CTA and
+    would need more shared memory than a CTA has, so the pass runs on the
+    per-output kernel; along axis 0 the column kernels take it."""
+    x = _rand((16, 100), dtype, seed=8)
+    w = np.random.default_rng(8001).random(8001).astype(np.float32) / 8001
+    xd = dev(x)
+    for axis in (0, 1):
+        for mode in ("nearest", "mirror", "constant"):
+            got = host(ndi.correlate1d(xd, w, axis, mode=mode, cval=2.0, output=np.float32))
+            exp = R.correlate1d(x, w, axis, mode=mode, cval=2.0, output=np.float32)
+            np.testing.assert_array_equal(got, exp, err_msg=f"axis={axis} mode={mode}")
+
+
 def test_nonfinite_inputs_and_zero_taps(ndi):
     """Zero taps are skipped by the elementwise kernel (3-D) but not by the
     shared-memory kernel (2-D): an inf under a zero tap differs."""
