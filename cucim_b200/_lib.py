@@ -86,6 +86,7 @@ _sigs = {
     "cimx_last_error_string": ([], ctypes.c_char_p),
     "cimx_set_allocator": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
     "cimx_device_status": ([ctypes.c_int], ctypes.c_int),
+    "cimx_wait_selftest": ([ctypes.c_int, ctypes.c_longlong, ctypes.c_void_p], ctypes.c_int),
     "cimx_correlate1d": (
         [_A, _A, _P(ctypes.c_double), ctypes.c_int, ctypes.c_int, ctypes.c_int,
          ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_void_p],

@@ -137,6 +137,8 @@ bool overlaps(const CimxArray* a, const CimxArray* b) {
   return numel(a) > 0 && numel(b) > 0 && a0 < b1 && b0 < a1;
 }
 
+}  // namespace
+
 int check_mode(int mode) {
   if (mode < CIMX_MODE_REFLECT || mode > CIMX_MODE_CONSTANT)
     return fail(CIMX_E_INVALID, "boundary mode not supported");
@@ -180,7 +182,6 @@ int make_pass(const CimxArray* shape_of, const CimxPass& p, std::vector<double>&
   return CIMX_OK;
 }
 
-}  // namespace
 }  // namespace cimx
 
 using namespace cimx;

@@ -6,6 +6,7 @@
 #include <stdint.h>
 
 #include <string>
+#include <vector>
 
 #include "../../include/cimx.h"
 
@@ -31,12 +32,22 @@ struct PassDesc {
   bool w64;        // weights type is float64
   bool cval_as_input;
   bool skip_zero;  // skip zero taps (only matters for non-finite inputs)
+  bool no_alloc;   // the pass must not take scratch memory (cimx_separable_noalloc)
   const double* taps;  // host taps, already flipped for convolution, not yet rounded
 };
 
 void set_error(const std::string& msg);
 int fail(int code, const std::string& msg);
 int cuda_fail(cudaError_t e, const char* what);
+
+// Argument checks shared by every entry point that takes a CimxPass list
+// (cimx_api.cu): the boundary mode, and one pass resolved against the shape of
+// `shape_of` into a PassDesc (taps copied into taps_store and flipped for
+// convolution, origin checked, anchor computed). in/out/dtypes are left for
+// the caller to fill.
+int check_mode(int mode);
+int make_pass(const CimxArray* shape_of, const CimxPass& p, std::vector<double>& taps_store,
+              PassDesc& d);
 
 // scratch memory through the installed allocator
 void* scratch_alloc(size_t nbytes, cudaStream_t s);

@@ -28,22 +28,51 @@ constexpr size_t kNoAllocScratchBytes = size_t(64) << 20;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
-// Host code cannot use g_noalloc_scratch's name as a device address: resolve
-// it once per device with that device current.
+// Host code cannot use g_noalloc_scratch's name as a device address: the
+// address is resolved with cudaGetSymbolAddress, with the device current, the
+// first time a device is used. The cache is keyed on the device's current
+// context as well, so that after cudaDeviceReset (which gives the module, and
+// the array, a new address in a new primary context) the address is resolved
+// again instead of reused.
+using CtxGetCurrentFn = int (*)(void**);  // cuCtxGetCurrent(CUcontext*)
+
+CtxGetCurrentFn ctx_get_current() {
+  static CtxGetCurrentFn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<CtxGetCurrentFn>(p);
+  });
+  return fn;
+}
+
+constexpr int kMaxDevices = 64;
 std::mutex g_mu;
-void* g_scratch_ptr[64] = {nullptr};
+void* g_scratch_ptr[kMaxDevices] = {nullptr};
+void* g_scratch_ctx[kMaxDevices] = {nullptr};
 
 int scratch_address(void** out) {
   int dev = -1;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
-  if (dev < 0 || dev >= 64) return fail(CIMX_E_INVALID, "device ordinal out of range");
+  if (dev < 0 || dev >= kMaxDevices) return fail(CIMX_E_INVALID, "device ordinal out of range");
+  CtxGetCurrentFn get = ctx_get_current();
+  if (!get) return fail(CIMX_E_CUDA, "cuCtxGetCurrent is not available");
+  // NULL before the runtime has made the device's primary context current
+  void* ctx = nullptr;
+  if (get(&ctx) != 0) return fail(CIMX_E_CUDA, "cuCtxGetCurrent failed");
   std::lock_guard<std::mutex> g(g_mu);
-  if (!g_scratch_ptr[dev]) {
+  if (!ctx || !g_scratch_ptr[dev] || g_scratch_ctx[dev] != ctx) {
+    // resolving the symbol also creates the primary context when needed
     void* p = nullptr;
     e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(no-allocation scratch)");
+    if (get(&ctx) != 0 || !ctx) return fail(CIMX_E_CUDA, "no current context");
     g_scratch_ptr[dev] = p;
+    g_scratch_ctx[dev] = ctx;
   }
   *out = g_scratch_ptr[dev];
   return CIMX_OK;
@@ -102,44 +131,15 @@ extern "C" CIMX_API int cimx_separable_noalloc(const CimxArray* in, const CimxAr
   std::vector<std::vector<double>> taps(npasses);
   std::vector<PassDesc> ds(npasses);
   for (int i = 0; i < npasses; ++i) {
-    const CimxPass& p = passes[i];
-    if (p.ntaps < 1 || !p.taps) return fail(CIMX_E_INVALID, "incorrect filter size");
-    int axis = p.axis < 0 ? p.axis + in->ndim : p.axis;
-    if (axis < 0 || axis >= in->ndim) return fail(CIMX_E_INVALID, "axis out of range");
-    if (p.mode < CIMX_MODE_REFLECT || p.mode > CIMX_MODE_CONSTANT)
-      return fail(CIMX_E_INVALID, "boundary mode not supported");
-    const int K = p.ntaps;
-    int origin = p.origin;
-    if (K / 2 + origin < 0 || K / 2 + origin >= K) return fail(CIMX_E_INVALID, "invalid origin");
-    const bool w64 = (p.flags & CIMX_F_W64) != 0;
-    const size_t max_taps = kParamTapBytes / (w64 ? sizeof(double) : sizeof(float));
-    if ((size_t)K > max_taps)
+    if ((rc = make_pass(in, passes[i], taps[i], ds[i]))) return rc;
+    const size_t max_taps = kParamTapBytes / (ds[i].w64 ? sizeof(double) : sizeof(float));
+    if ((size_t)ds[i].K > max_taps)
       return fail(CIMX_E_INVALID,
-                  "cimx_separable_noalloc: a pass has " + std::to_string(K) +
+                  "cimx_separable_noalloc: a pass has " + std::to_string(ds[i].K) +
                       " taps; without scratch memory at most " + std::to_string(max_taps) +
                       " fit in the launch parameters");
-    taps[i].assign(p.taps, p.taps + K);
-    if (p.flags & CIMX_F_CONVOLVE) {
-      std::reverse(taps[i].begin(), taps[i].end());
-      origin = -origin;
-      if (K % 2 == 0) origin -= 1;
-    }
-    PassDesc& d = ds[i];
-    d = PassDesc{};
-    d.outer = 1;
-    for (int k = 0; k < axis; ++k) d.outer *= in->shape[k];
-    d.L = in->shape[axis];
-    d.inner = 1;
-    for (int k = axis + 1; k < in->ndim; ++k) d.inner *= in->shape[k];
-    d.axis = axis;
-    d.K = K;
-    d.anchor = K / 2 + origin;
-    d.mode = p.mode;
-    d.cval = p.cval;
-    d.w64 = w64;
-    d.cval_as_input = (p.flags & CIMX_F_CVAL_AS_INPUT) != 0;
-    d.skip_zero = (p.flags & CIMX_F_SKIP_ZERO_TAPS) != 0;
-    d.taps = taps[i].data();
+    // a pass whose taps would have to go to device memory fails instead
+    ds[i].no_alloc = true;
   }
   const size_t need = npasses > 1 ? (size_t)n * dtype_size(out->dtype) : 0;
   if (need > kNoAllocScratchBytes)

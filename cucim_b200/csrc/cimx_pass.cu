@@ -557,6 +557,11 @@ int launch_w(const PassDesc& d, cudaStream_t st) {
   if (fits_param && !direct) {
     std::copy(w.begin() + lo, w.begin() + hi, tb.w);
   } else {
+    if (d.no_alloc)
+      return fail(CIMX_E_INVALID,
+                  "this pass needs device scratch memory for its " + std::to_string(K) +
+                      " taps (beyond the launch parameters or the shared-memory budget), "
+                      "which an entry point that allocates nothing cannot take");
     gt = scratch_alloc(gbytes, st);
     if (!gt) return fail(CIMX_E_NOMEM, "scratch allocation for taps failed");
     cudaError_t e = cudaMemcpyAsync(gt, w.data() + lo, sizeof(W) * K, cudaMemcpyHostToDevice, st);

@@ -109,16 +109,17 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
 }
 
-// Bounded wait; false on timeout (recorded) or when another role aborted.
+// Bounded wait (`limit_ns` of %globaltimer); false on timeout (recorded) or
+// when another role aborted.
 __device__ __noinline__ bool wait_bar(uint64_t* bar, uint32_t parity, volatile int* abort_flag,
-                                      int* status) {
+                                      int* status, uint64_t limit_ns = kTcsWaitNs) {
   if (mbar_try_wait(bar, parity)) return true;
   const uint64_t t0 = gtimer();
   for (uint32_t i = 1;; ++i) {
     if (mbar_try_wait(bar, parity)) return true;
     if ((i & 255u) == 0) {
       if (abort_flag && *abort_flag) return false;
-      if (gtimer() - t0 > kTcsWaitNs) {
+      if (gtimer() - t0 > limit_ns) {
         if (abort_flag) *abort_flag = 1;
         if (status) atomicExch(status, -6 /* CIMX_E_TIMEOUT */);
         return false;
@@ -764,3 +765,46 @@ int launch_tcs_pass(const PassDesc& d, cudaStream_t st) {
 }
 
 }  // namespace cimx
+
+// ------------------------------------------------ bounded-wait self-test
+//
+// One CTA, one thread: an mbarrier expecting one arrival that nothing ever
+// makes, waited on with the same helpers the TMA-fed kernels use (poll-count
+// bound, `which` 0) or the tensor-core pass uses (%globaltimer bound, `which`
+// 1). The wait runs out after `limit` polls / nanoseconds, records
+// CIMX_E_TIMEOUT in the device status word and the kernel returns; no copy or
+// MMA is in flight, so the context stays usable.
+namespace cimx {
+namespace {
+
+__global__ void k_wait_selftest(int which, long long limit, int* status) {
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ int abort_flag;
+  if (threadIdx.x != 0) return;
+  mbar_init(&bar, 1);
+  abort_flag = 0;
+  mbar_fence_init();
+  bool ok;
+  if (which == 0)
+    ok = mbar_wait(&bar, 0, status, limit);
+  else
+    ok = wait_bar(&bar, 0, &abort_flag, status, (uint64_t)limit);
+  // the barrier cannot have completed: nothing arrived on it
+  if (ok && status) atomicExch(status, -1 /* CIMX_E_INVALID: the wait did not run out */);
+}
+
+}  // namespace
+}  // namespace cimx
+
+extern "C" CIMX_API int cimx_wait_selftest(int which, long long limit, void* stream) {
+  using namespace cimx;
+  if (which != 0 && which != 1) return fail(CIMX_E_INVALID, "which must be 0 or 1");
+  // at most 2^24 polls or 0.1 s: the self-test must end quickly
+  const long long cap = which == 0 ? (1ll << 24) : 100000000ll;
+  if (limit < 1 || limit > cap)
+    return fail(CIMX_E_INVALID, "limit out of range (1.." + std::to_string(cap) + ")");
+  int* status = device_status_word();
+  if (!status) return fail(CIMX_E_CUDA, "no device status word");
+  k_wait_selftest<<<1, 32, 0, static_cast<cudaStream_t>(stream)>>>(which, limit, status);
+  return cuda_fail(cudaGetLastError(), "wait self-test launch");
+}

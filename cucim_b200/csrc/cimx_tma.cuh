@@ -52,10 +52,11 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t phase) {
 }
 
 // Bounded wait for `phase` of an mbarrier. Returns false (and records
-// CIMX_E_TIMEOUT in *status) if the barrier did not complete within the
-// poll limit.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase, int* status) {
-  for (long long i = 0; i < kWaitLimit; ++i)
+// CIMX_E_TIMEOUT in *status) if the barrier did not complete within `limit`
+// polls (kWaitLimit in the kernels; cimx_wait_selftest passes a small one).
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase, int* status,
+                                          long long limit = kWaitLimit) {
+  for (long long i = 0; i < limit; ++i)
     if (mbar_try_wait(bar, phase)) return true;
   if (status) atomicExch(status, -6 /* CIMX_E_TIMEOUT */);
   return false;

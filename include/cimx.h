@@ -119,6 +119,15 @@ CIMX_API const char* cimx_last_error_string(void);
  * kernels have no device-side waits. */
 CIMX_API int cimx_device_status(int clear);
 
+/* Self-test of the device-side timeout path. Launches one thread that waits
+ * on an mbarrier nothing arrives on, with the bounded wait of the TMA-fed
+ * kernels (which 0: `limit` polls, 1..2^24) or of the tensor-core pass
+ * (which 1: `limit` nanoseconds of %globaltimer, 1..1e8). The wait runs
+ * out, records CIMX_E_TIMEOUT in the status word read by
+ * cimx_device_status() and the kernel returns, leaving the context usable.
+ * No counterpart in cuCIM, whose kernels have no device-side waits. */
+CIMX_API int cimx_wait_selftest(int which, long long limit, void* stream);
+
 /* Scratch allocator hook (default: cudaMallocAsync / cudaFreeAsync on the
  * call's stream). Both functions receive the stream the call runs on. */
 typedef void* (*cimx_alloc_fn)(size_t nbytes, void* stream, void* user);
@@ -149,16 +158,20 @@ CIMX_API int cimx_separable(const CimxArray* in, const CimxArray* out, const Cim
  * running inside someone else's stream capture, plug-ins whose host
  * application owns every allocation, pipelines that forbid allocation after
  * start-up). No counterpart in cuCIM: it is an addition of this library.
- * Same arguments and results as cimx_separable, but the passes run one
- * launch each and the ping-pong intermediate lives in a 64 MiB static device
- * array that every GPU loading the library holds until exit; the call makes
- * no cudaMalloc/cudaFree or other allocating call. Limits: the intermediate
- * (element count x output itemsize, needed when npasses >= 2) must fit in
- * 64 MiB and each pass may have at most 1024 float32 / 512 float64 taps;
- * larger requests return CIMX_E_INVALID with a message. The first call on a
- * device resolves the array's device address (cudaGetSymbolAddress) and
- * should come before any stream capture. All calls share the one array:
- * calls that overlap on the GPU (concurrent streams) race on it. */
+ * The same arguments as cimx_separable except lib_flags; the results equal
+ * cimx_separable's with CIMX_L_NO_FUSION and no tensor flags, because the
+ * passes always run on the generic kernels, one launch each. The ping-pong
+ * intermediate lives in a 64 MiB static device array that every GPU loading
+ * the library holds until exit; the call makes no cudaMalloc/cudaFree or
+ * other allocating call. Limits: the intermediate (element count x output
+ * itemsize, needed when npasses >= 2) must fit in 64 MiB and each pass may
+ * have at most 1024 float32 / 512 float64 taps; larger requests, and a pass
+ * whose taps would need device memory, return CIMX_E_INVALID with a
+ * message. The first call on a device (and the first after cudaDeviceReset)
+ * resolves the array's device address (cudaGetSymbolAddress) and should come
+ * before any stream capture. All calls share the one array, which keeps the
+ * last call's contents: calls that overlap on the GPU (concurrent streams)
+ * race on it. */
 CIMX_API int cimx_separable_noalloc(const CimxArray* in, const CimxArray* out,
                                     const CimxPass* passes, int npasses, void* stream);
 

@@ -118,3 +118,41 @@ def test_modes_and_axes_checks():
         _util.check_axes((0, 0), 2)
     assert _util.check_axes(-1, 3) == (-1,)  # scalars are not normalised (UTIL:114-115)
     assert _util.check_axes([-1], 3) == (2,)
+
+
+_ALLOC = ctypes.CFUNCTYPE(ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_void_p)
+_FREE = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p,
+                         ctypes.c_void_p)
+
+
+def test_refused_scratch_allocation_is_e_nomem_and_memory_error():
+    """An allocator hook that returns NULL: a multi-pass call that needs the
+    ping-pong buffer fails with CIMX_E_NOMEM before any device work (the
+    pointers here are fake), and the Python layer turns it into MemoryError."""
+    calls = []
+    alloc = _ALLOC(lambda n, s, u: calls.append(n) or None)
+    free = _FREE(lambda p, n, s, u: None)
+    _lib.lib.cimx_set_allocator(ctypes.cast(alloc, ctypes.c_void_p),
+                                ctypes.cast(free, ctypes.c_void_p), None)
+    try:
+        a_in = _arr((6, 7), np.float32, 0x1000)
+        a_out = _arr((6, 7), np.float32, 0x9000)
+        t, p = _lib.taps_pointer(np.ones(3))
+        passes = (_lib.CimxPass * 2)()
+        for i in range(2):
+            passes[i].axis, passes[i].ntaps, passes[i].mode, passes[i].taps = i, 3, 0, p
+        rc = _lib.lib.cimx_separable(ctypes.byref(a_in), ctypes.byref(a_out), passes, 2,
+                                     _lib.L_NO_FUSION, None)
+        assert rc == _lib.E_NOMEM
+        assert calls == [6 * 7 * 4]
+        with pytest.raises(MemoryError):
+            _lib.check(rc, "separable")
+    finally:
+        _lib.lib.cimx_set_allocator(None, None, None)
+
+
+def test_wait_selftest_rejects_bad_arguments():
+    assert _lib.lib.cimx_wait_selftest(2, 10, None) == _lib.E_INVALID
+    assert _lib.lib.cimx_wait_selftest(0, 0, None) == _lib.E_INVALID
+    assert _lib.lib.cimx_wait_selftest(0, 1 << 25, None) == _lib.E_INVALID
+    assert _lib.lib.cimx_wait_selftest(1, 10 ** 9, None) == _lib.E_INVALID
