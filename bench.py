@@ -1,7 +1,8 @@
 """Benchmark of the separable filtering path on B200.
 
 Workload (one step): the 512 x 1024 x 1024 uint16 stack (smoothed noise with
-Poisson shot noise, seed 1) filtered by
+Poisson shot noise, seed 1; drawn slice by slice so that the CPU arm can
+regenerate any z-window of it exactly) filtered by
   - ndimage.gaussian_filter(sigma=(1, 2, 2), mode='mirror', output=float32),
   - ndimage.sobel(axis=a, output=float32) for a = 0, 1, 2,
   - ndimage.uniform_filter(size=5, output=uint16)  (bit-exact integer path),
@@ -41,9 +42,19 @@ three public calls per tile and once as one persistent launch replayed from
 a CUDA graph; the ratio of the two times, and a bit-for-bit comparison of
 the two outputs on a sample of tiles.
 
+Parity (reported in `parity`): after timing, the step's outputs are checked
+against the oracle on three 16-slice z-windows of the stack (first, middle,
+last; the oracle filters each window with its z halo), bit for bit; the
+first 8 slices of the stack are compared with the CPU arm's regeneration of
+them; the 2-D gaussian of the 2048 x 2048 image is checked bit for bit; the
+precision-path errors are pointwise over the full 8192 x 8192 image; the
+frangi output on the 256^3 volume is compared with the oracle's.
+
 --impl reference times the CPU restatement of cuCIM's arithmetic (the
 oracle; cuCIM itself needs CuPy and has no CPU implementation) on the host
-cores, on a bounded slab of the same stack.
+cores, on the first 8 z-slices of the same stack (regenerated on the CPU by
+the same generator), with the same `config`. It imports nothing from the
+cucim_b200 package: the generators are loaded from their file.
 
 Multi-GPU: the path has no exchange step; N ranks run N independent replicas
 of the step (weak scaling) and the time is the max over ranks.
@@ -83,27 +94,48 @@ def parse():
     p.add_argument("--tiles", type=int, default=4096, help="tiles in the batched-tiles report")
     p.add_argument("--no-frangi", action="store_true", help="skip the frangi report")
     p.add_argument("--no-plain2d", action="store_true", help="skip the 2-D gaussian report")
+    p.add_argument("--no-parity", action="store_true",
+                   help="skip the oracle checks of the outputs (parity field)")
     return p.parse_args()
 
 
 # ------------------------------------------------------------------ inputs
 
+def load_synthetic():
+    """The input generators (numpy only), loaded from their file so that the
+    CPU arm never runs cucim_b200/__init__.py, which loads libcimx.so."""
+    import importlib.util
+
+    path = os.path.join(ROOT, "cucim_b200", "synthetic.py")
+    spec = importlib.util.spec_from_file_location("cimx_bench_synthetic", path)
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
 def make_stack(shape, device):
-    """Seed-1 stack: normal noise smoothed with sigma 3, rescaled to [0, 65535],
-    Poisson shot noise, clipped, uint16 (generated on the device)."""
+    """The seed-1 stack: per-slice normal noise (host), smoothed on the device
+    by gaussian_filter(sigma 3, reflect), mapped to [0, 65535] with Poisson
+    shot noise per slice (host), uploaded as uint16."""
     import torch
 
     from cucim_b200 import ndimage as ndi
 
-    g = torch.Generator(device=device).manual_seed(1)
-    noise = torch.randn(shape, generator=g, device=device, dtype=torch.float32)
-    sm = ndi.gaussian_filter(noise, 3.0, mode="reflect")
+    S = load_synthetic()
+    noise = torch.from_numpy(S.stack_noise(range(shape[0]), shape[1:])).to(device)
+    sm = ndi.gaussian_filter(noise, S.STACK_SIGMA, mode="reflect", truncate=S.STACK_TRUNCATE)
     del noise
-    lo, hi = sm.min(), sm.max()
-    sm.sub_(lo).mul_(65535.0 / (hi - lo))
-    shot = torch.poisson(sm, generator=g)
+    smh = sm.cpu().numpy()
     del sm
-    return shot.clamp_(0, 65535).to(torch.int32).to(torch.uint16)
+    return torch.from_numpy(S.stack_shot(smh, range(shape[0]))).to(device)
+
+
+def stack_config(shape, world):
+    """The `config` of both arms (the CPU arm states its sample separately)."""
+    return {"workload": "3-D uint16 stack (seed 1): gaussian(sigma=(1,2,2), mirror)->f32, "
+                        "sobel(axis=0,1,2)->f32, uniform(size=5)->u16 (bit-exact)",
+            "shape": list(shape), "voxels_per_step": int(np.prod(shape)),
+            "l2": "inputs 1 GiB > L2 (126 MB), no flush", "parallelism": f"replicas x{world}"}
 
 
 # --------------------------------------------------------------- clocks
@@ -285,6 +317,12 @@ def run_ours(args, rank, world, local_rank):
     if not args.no_e2e:
         e2e = run_e2e(ndi, torch, x, shape, outs, args, world)
 
+    parity = None
+    if rank == 0 and not args.no_parity:
+        step_ops(ndi, x, outs)  # the per-kernel timing above rewrote some outputs
+        torch.cuda.synchronize()
+        parity = stack_parity(x, outs)
+
     x_host = x.cpu() if rank == 0 else None
     prec = None
     if rank == 0 and not args.no_precision:
@@ -305,8 +343,54 @@ def run_ours(args, rank, world, local_rank):
         p2 = run_plain2d(torch, dev, hbm_gbs=_peaks().get("hbm_gbs"))
 
     return {"value": value, "ms": ms, "nvox": nvox, "kernels": kres, "clocks": clk.summary(),
-            "e2e": e2e, "x": x_host, "precision": prec, "tiles": tiles, "frangi": fr,
+            "e2e": e2e, "x": x_host, "parity": parity, "precision": prec, "tiles": tiles, "frangi": fr,
             "plain2d": p2}
+
+
+# the z radius of the step's filters: gaussian sigma 1 (4), sobel (1), uniform 5 (2)
+STEP_Z_HALO = 4
+ORACLE_STEP = (
+    lambda R, x: R.gaussian_filter(x, (1, 2, 2), mode="mirror", output=np.float32),
+    lambda R, x: R.sobel(x, 0, output=np.float32),
+    lambda R, x: R.sobel(x, 1, output=np.float32),
+    lambda R, x: R.sobel(x, 2, output=np.float32),
+    lambda R, x: R.uniform_filter(x, 5, output=np.uint16),
+)
+STEP_NAMES = ("gaussian_f32", "sobel0_f32", "sobel1_f32", "sobel2_f32", "uniform5_u16")
+
+
+def stack_parity(x, outs, win=16, sample=8):
+    """The step's outputs against the oracle on the first, middle and last
+    `win` z-slices of the stack: the oracle filters each window with
+    STEP_Z_HALO extra slices on each side (none beyond the stack's ends,
+    where the boundary mode applies as on the full stack) and the window's
+    own slices are compared bit for bit. Also: the first `sample` slices of
+    the stack against the CPU arm's regeneration of them."""
+    from oracle import restate as R
+
+    R.THREADS = os.cpu_count() or 1
+    Z = x.shape[0]
+    t0 = time.perf_counter()
+    windows = []
+    for z0 in sorted({0, max(0, Z // 2 - win // 2), max(0, Z - win)}):
+        z1 = min(Z, z0 + win)
+        a, b = max(0, z0 - STEP_Z_HALO), min(Z, z1 + STEP_Z_HALO)
+        xs = x[a:b].cpu().numpy()
+        row = {"z": [z0, z1]}
+        for name, op, o in zip(STEP_NAMES, ORACLE_STEP, outs):
+            exp = op(R, xs)[z0 - a:z1 - a]
+            got = o[z0:z1].cpu().numpy()
+            row[name] = bool(np.array_equal(got, exp))
+        windows.append(row)
+    S = load_synthetic()
+    regen = S.stack_window(0, sample, tuple(x.shape), R.gaussian_filter)
+    same_input = bool(np.array_equal(regen, x[:sample].cpu().numpy()))
+    return {"check": f"oracle bit for bit on {len(windows)} z-windows of {win} slices "
+                     f"(each with a {STEP_Z_HALO}-slice halo), all five filters",
+            "windows": windows,
+            "bit_exact": all(all(v for k, v in w.items() if k != "z") for w in windows),
+            "input_equals_cpu_arm_sample": same_input,
+            "seconds": time.perf_counter() - t0}
 
 
 def run_e2e(ndi, torch, x, shape, douts, args, world):
@@ -397,57 +481,87 @@ def tf32x3_flops_per_output(K):
     return 3 * 16 * sb
 
 
-def run_precision(torch, ndi, dev, reps=5, crop=2048, size=8192, tf32_peak=None):
+def run_precision(torch, ndi, dev, reps=5, crop=2048, size=8192, tf32_peak=None, floor=1e-3):
     """Plain float32 vs TF32x3 tensor-core filters on the precision workload:
-    device time per filter (CUDA events, `reps` repetitions after a warm-up),
-    and the error of each against float64 on a crop."""
+    device time per filter (CUDA events, `reps` repetitions after a warm-up)
+    and the error of each result over the FULL image against a float64
+    reference. The reference is the same filter computed in float64 on the
+    device (float64 taps, float64 fused chain: its own error is ~1e-15); it
+    is pinned against scipy.ndimage in float64 on a crop, which it must match
+    to 1e-12. Errors are pointwise: |out - ref| / max(|ref|, floor); every
+    output of this workload is positive and far above the floor (counted in
+    `pixels_below_floor`). The error relative to the largest output is given
+    beside it."""
     import scipy.ndimage as sndi
 
-    from cucim_b200 import synthetic
-
-    img = synthetic.rectangles_image((size, size), n_rect=64, seed=2)
+    S = load_synthetic()
+    img = S.rectangles_image((size, size), n_rect=64, seed=2)
     X = torch.as_tensor(img).to(dev)
     O = torch.empty_like(X)
+    X64 = X.double()
     crop = min(crop, size)
-    xc = np.ascontiguousarray(img[:crop, :crop])
-    Xc = torch.as_tensor(xc).to(dev)
+    xc = np.ascontiguousarray(img[:crop, :crop]).astype(np.float64)
+    Xc64 = torch.as_tensor(xc).to(dev)
     res = {}
     for name, fn, kw, K in PRECISION_OPS:
         f = getattr(ndi, fn)
-        row = {}
-        ref = getattr(sndi, fn)(xc.astype(np.float64), mode="nearest", **kw)
-        scale = float(np.abs(ref).max())
+        ref = f(X64, mode="nearest", **kw)
+        sref = getattr(sndi, fn)(xc, mode="nearest", **kw)
+        pin = float(np.abs(f(Xc64, mode="nearest", **kw).cpu().numpy() - sref).max()
+                    / np.abs(sref).max())
+        aref = ref.abs()
+        den = aref.clamp_min(floor)
+        row = {"reference_vs_scipy_f64_on_crop": pin}
         for algo, key in ((None, "plain_f32"), ("tensor", "tensor_tf32x3")):
             ms = time_kernel(lambda: f(X, mode="nearest", output=O, algorithm=algo, **kw), reps, torch)
-            got = f(Xc, mode="nearest", algorithm=algo, **kw).cpu().numpy().astype(np.float64)
-            err = np.abs(got - ref)
+            f(X, mode="nearest", output=O, algorithm=algo, **kw)
+            err = (O.double() - ref).abs()
+            rel = err / den
             row[key] = {"ms": ms, "gpx_s": X.numel() / (ms * 1e-3) / 1e9,
-                        "max_rel_err": float(err.max() / scale),
-                        "mean_rel_err": float(err.mean() / scale)}
+                        "max_rel_err": float(rel.max()), "mean_rel_err": float(rel.mean()),
+                        "max_err_over_max_output": float(err.max() / aref.max())}
+            del err, rel
+        row["pixels_below_floor"] = int((aref < floor).sum())
         row["speedup"] = row["plain_f32"]["ms"] / row["tensor_tf32x3"]["ms"]
         tflops = 2 * tf32x3_flops_per_output(K) * X.numel() / (row["tensor_tf32x3"]["ms"] * 1e-3) / 1e12
         row["tensor_tf32x3"]["executed_tflops"] = tflops
-        row["tensor_tf32x3"]["useful_tflops"] = (2 * 2 * 2 * K * X.numel()
-                                                 / (row["tensor_tf32x3"]["ms"] * 1e-3) / 1e12)
+        # two passes of K fused multiply-adds (2 flops each) per pixel
+        for key in ("plain_f32", "tensor_tf32x3"):
+            row[key]["useful_tflops"] = 2 * 2 * K * X.numel() / (row[key]["ms"] * 1e-3) / 1e12
         if tf32_peak:
             row["tensor_tf32x3"]["frac_of_tf32_peak"] = tflops / tf32_peak
         row["tensor_within_2e-6"] = row["tensor_tf32x3"]["max_rel_err"] <= 2e-6
+        row["plain_within_2e-6"] = row["plain_f32"]["max_rel_err"] <= 2e-6
         res[name] = row
+        del ref, aref, den
+    # the oracle's sigma-16 gaussian on the crop with all host threads: the CPU baseline
+    from oracle import restate as R
+
+    R.THREADS = os.cpu_count() or 1
+    xc32 = xc.astype(np.float32)
+    t0 = time.perf_counter()
+    R.gaussian_filter(xc32, 16.0, mode="nearest")
+    cpu_s = time.perf_counter() - t0
     return {"workload": f"float32 {size}x{size} uniform noise + 64 rectangles (seed 2), mode nearest",
+            "cpu_baseline": {"value": xc32.size / cpu_s / 1e9, "unit": "Gpx/s",
+                             "cores": R.THREADS, "kind": "port",
+                             "sample": f"gaussian sigma 16 (float32 chain) on the {crop}x{crop} "
+                                       f"crop, {cpu_s:.2f} s"},
             "tf32_peak_tflops": tf32_peak,
             "tf32_peak_source": "half the measured bf16 dense peak (kind::tf32 MMAs ran at "
                                 "4092 vs 8184 flop/clk/SM for kind::f16 in a microbenchmark)",
-            "error_reference": f"scipy.ndimage float64 on the {crop}x{crop} crop; "
-                               "error = |out - ref| / max|ref|",
-            "filters": res}
+            "error_reference": f"the filter in float64 on the device over the full {size}x{size} "
+                               f"image, pinned against scipy.ndimage float64 on the {crop}x{crop} "
+                               "crop; error = |out - ref| / max(|ref|, floor)",
+            "floor": floor, "filters": res}
 
 
 # ----------------------------------------------------------- batched tiles
 
 def run_tiles(torch, dev, reps=3, check=64, n_tiles=4096):
-    from cucim_b200 import batch, synthetic
+    from cucim_b200 import batch
 
-    tiles, sigmas = synthetic.rgb_tiles_device(dev, n_tiles=n_tiles)
+    tiles, sigmas = load_synthetic().rgb_tiles_device(dev, n_tiles=n_tiles)
     npx = sum(int(t.shape[0]) * int(t.shape[1]) for t in tiles)
     b = batch.TileBatch(tiles, sigmas)
     g = b.graph()
@@ -472,12 +586,28 @@ def run_tiles(torch, dev, reps=3, check=64, n_tiles=4096):
     ms_t = s.elapsed_time(e)
     step = max(1, len(tiles) // check)
     same = all(torch.equal(b.outputs[i], ref[i]) for i in range(0, len(tiles), step))
+    # the oracle on a sample of tiles: bit for bit, and its time as the CPU baseline
+    from oracle import restate as R
+
+    R.THREADS = os.cpu_count() or 1
+    sample = list(range(0, len(tiles), max(1, len(tiles) // 16)))[:16]
+    host = [tiles[i].cpu().numpy() for i in sample]
+    t0 = time.perf_counter()
+    exp = [R.sk_sobel(R.sk_gaussian(R.rgb2gray(h), sigmas[i])) for h, i in zip(host, sample)]
+    cpu_s = time.perf_counter() - t0
+    spx = sum(h.shape[0] * h.shape[1] for h in host)
+    oracle_ok = all(np.array_equal(b.outputs[i].cpu().numpy(), e) for i, e in zip(sample, exp))
     return {"workload": f"{len(tiles)} uint8 RGB tiles, sides 64..1024 (seed 3), "
                         "rgb2gray -> gaussian(sigma 0.5..8, nearest) -> sobel magnitude, float32 out",
             "pixels": npx, "batched_ms": ms_b, "batched_gpx_s": npx / (ms_b * 1e-3) / 1e9,
             "per_tile_ms": ms_t, "per_tile_gpx_s": npx / (ms_t * 1e-3) / 1e9,
             "speedup": ms_t / ms_b, "launches_batched": 1, "launches_per_tile": "about 7 per tile",
-            "bit_identical": bool(same), "tiles_compared": len(range(0, len(tiles), step))}
+            "bit_identical": bool(same), "tiles_compared": len(range(0, len(tiles), step)),
+            "oracle_bit_exact": bool(oracle_ok), "oracle_tiles_compared": len(sample),
+            "cpu_baseline": {"value": spx / cpu_s / 1e9, "unit": "Gpx/s", "cores": R.THREADS,
+                             "kind": "port",
+                             "sample": f"{len(sample)} tiles ({spx} px), rgb2gray -> gaussian -> "
+                                       f"sobel in the oracle, {cpu_s:.2f} s"}}
 
 
 # ---------------------------------------------------------- plain 2-D case
@@ -487,10 +617,10 @@ def run_plain2d(torch, dev, n_img=16, reps=5, hbm_gbs=None):
     float32 2048 x 2048 uniform images (seed 0): two fused passes of 33 taps.
     One image is 16 MiB and would stay in L2, so each timed repetition
     filters 16 distinct images (512 MiB in and out)."""
-    from cucim_b200 import synthetic
     from cucim_b200.skimage import filters
 
-    base = torch.as_tensor(synthetic.uniform_image((2048, 2048), seed=0)).to(dev)
+    S = load_synthetic()
+    base = torch.as_tensor(S.uniform_image((2048, 2048), seed=0)).to(dev)
     imgs = [base + float(i) for i in range(n_img)]
     outs = [torch.empty_like(base) for _ in range(n_img)]
 
@@ -515,6 +645,16 @@ def run_plain2d(torch, dev, n_img=16, reps=5, hbm_gbs=None):
     ms = time_kernel(one_direct, reps, torch) / n_img
     ms_api = time_kernel(one, reps, torch) / n_img
     ms_kernel = time_kernel(one_stack, reps, torch) / n_img
+    # the 2048 x 2048 image against the oracle, bit for bit, and the oracle's
+    # time on it with all host threads as the CPU baseline
+    from oracle import restate as R
+
+    R.THREADS = os.cpu_count() or 1
+    img = S.uniform_image((2048, 2048), seed=0)
+    got = filters.gaussian(base, sigma=4.0, mode="reflect", truncate=4.0).cpu().numpy()
+    t0 = time.perf_counter()
+    exp = R.sk_gaussian(img, 4.0, mode="reflect", truncate=4.0)
+    cpu_s = time.perf_counter() - t0
     gbs = 8 * base.numel() / (ms_kernel * 1e-3) / 1e9
     res = {"workload": "float32 2048x2048 uniform (seed 0), gaussian sigma 4 (K=33), mode reflect; "
                        f"{n_img} distinct images per repetition (inputs above L2)",
@@ -522,7 +662,10 @@ def run_plain2d(torch, dev, n_img=16, reps=5, hbm_gbs=None):
            "gb_s": gbs, "kernel_note": f"one launch over the {n_img} images as a stack, axes (1, 2)",
            "ms_per_image_per_call": ms, "ms_per_image_skimage_api": ms_api,
            "per_call_note": "one ndimage.gaussian_filter call per image (includes the host work "
-                            "of each call) and one skimage.filters.gaussian call per image"}
+                            "of each call) and one skimage.filters.gaussian call per image",
+           "oracle_bit_exact": bool(np.array_equal(got, exp)),
+           "cpu_baseline": {"value": img.size / cpu_s / 1e9, "unit": "Gpx/s", "cores": R.THREADS,
+                            "kind": "port", "sample": f"the 2048x2048 image, {cpu_s:.3f} s"}}
     if hbm_gbs:
         res["frac_of_hbm"] = gbs / hbm_gbs
     # 33 taps on each of two axes: 2 * 2 * 33 useful flops per pixel, which
@@ -538,18 +681,39 @@ def run_plain2d(torch, dev, n_img=16, reps=5, hbm_gbs=None):
 
 # --------------------------------------------------------------- frangi
 
-def run_frangi(torch, dev, reps=3):
+def frangi_agreement(got, exp):
+    """How far the GPU frangi output is from the oracle's: the share of
+    voxels that differ, the largest difference in float32 ulps (of the
+    oracle's value) and relative to the largest output, and the largest
+    pointwise relative difference among outputs above 1e-3 of the largest."""
+    g = got.astype(np.float64)
+    e = exp.astype(np.float64)
+    diff = np.abs(g - e)
+    scale = float(np.abs(e).max()) or 1.0
+    ulp = np.spacing(np.abs(exp).astype(np.float32)).astype(np.float64)
+    big = np.abs(e) >= 1e-3 * scale
+    return {"voxels": int(e.size), "voxels_differing": int((diff > 0).sum()),
+            "max_ulps": float((diff / ulp).max()),
+            "max_diff_over_max_output": float(diff.max() / scale),
+            "max_rel_diff_outputs_above_1e-3_of_max": float((diff[big] / np.abs(e[big])).max())
+            if big.any() else 0.0,
+            "nan_mismatch": int((np.isnan(g) != np.isnan(e)).sum())}
+
+
+def run_frangi(torch, dev, reps=3, check=True):
     """Multi-scale frangi (sigmas 1..5, alpha = beta = 0.5, automatic gamma,
     black_ridges=False) on the seed-4 segments volume: plain float32 passes
     against algorithm="tensor" (which keeps the plain kernels on these
     256-sample lines, where they measured faster) and against the tensor
     cores forced onto every pass, with the largest difference to the plain
-    result relative to the largest output."""
+    result relative to the largest output; the plain result against the
+    oracle's frangi on the same volume, whose time with all host threads is
+    the CPU baseline."""
     from cucim_b200 import ndimage as ndi
-    from cucim_b200 import synthetic
     from cucim_b200.skimage import filters
 
-    vol = torch.as_tensor(synthetic.segments_volume((256, 256, 256), seed=4)).to(dev)
+    vol_h = load_synthetic().segments_volume((256, 256, 256), seed=4)
+    vol = torch.as_tensor(vol_h).to(dev)
     kw = dict(sigmas=range(1, 6), alpha=0.5, beta=0.5, gamma=None, black_ridges=False)
     res = {}
     outs = {}
@@ -570,16 +734,29 @@ def run_frangi(torch, dev, reps=3):
         res[key]["speedup"] = res["plain_f32"]["ms"] / res[key]["ms"]
         res[key]["vs_plain_max_rel"] = float((t - p).abs().max()) / scale
         res[key]["vs_plain_mean_rel"] = float((t - p).abs().mean()) / scale
-    return {"workload": "float32 256^3 segments volume (seed 4), frangi sigmas 1..5, "
-                        "27 Gaussian-derivative passes per sigma (taps 143, 23, 35, 47, 57)",
-            **res}
+    out = {"workload": "float32 256^3 segments volume (seed 4), frangi sigmas 1..5, "
+                       "27 Gaussian-derivative passes per sigma (taps 143, 23, 35, 47, 57)",
+           **res}
+    if check:
+        from oracle import restate as R
+
+        R.THREADS = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        exp = R.frangi(vol_h, **kw)
+        cpu_s = time.perf_counter() - t0
+        out["oracle"] = frangi_agreement(outs["plain_f32"].cpu().numpy(), exp)
+        out["cpu_baseline"] = {"value": vol_h.size / cpu_s / 1e9, "unit": "Gvox/s",
+                               "cores": R.THREADS, "kind": "port",
+                               "sample": f"the whole 256^3 volume, {cpu_s:.1f} s"}
+    return out
 
 
 # ------------------------------------------------------------- CPU leg
 
-def cpu_baseline(x_host, slab_z=16, threads=None):
+def cpu_baseline(x_host, slab_z=8, threads=None):
     """The oracle (exact restatement of cuCIM's arithmetic, C + OpenMP) on a
-    slab of the stack: z-slab of `slab_z` slices with the full y, x extent."""
+    slab of the stack: the first `slab_z` z-slices with the full y, x extent
+    (the CPU arm's sample)."""
     from oracle import restate as R
 
     threads = threads or os.cpu_count() or 1
@@ -595,23 +772,23 @@ def cpu_baseline(x_host, slab_z=16, threads=None):
             "sample": f"z-slab {xs.shape} of the stack, all five filters, {dt:.2f} s"}
 
 
-def run_reference(args):
-    """CPU arm: the oracle on the host cores, same workload and metric."""
+def run_reference(args, world):
+    """CPU arm: the oracle on the host cores, same workload, metric and
+    config; each step filters the first 8 z-slices of the stack (regenerated
+    on the CPU by the same generator: bit-identical to those slices of the
+    GPU arm's stack). Imports nothing from the cucim_b200 package."""
     shape = tuple(int(v) for v in args.shape.split(",")) if args.shape else SHAPE
-    from cucim_b200 import synthetic
-
-    # the slab the CPU filters per step: 8 z-slices of a seed-1 stack
-    xs = synthetic.smooth_volume_u16((8,) + shape[1:], seed=1)
     from oracle import restate as R
 
     threads = os.cpu_count() or 1
     R.THREADS = threads
+    S = load_synthetic()
+    sample_z = min(8, shape[0])
+    xs = S.stack_window(0, sample_z, shape, R.gaussian_filter)
 
     def step():
-        R.gaussian_filter(xs, (1, 2, 2), mode="mirror", output=np.float32)
-        for a in range(3):
-            R.sobel(xs, a, output=np.float32)
-        R.uniform_filter(xs, 5, output=np.uint16)
+        for op in ORACLE_STEP:
+            op(R, xs)
 
     for _ in range(args.warmup):
         step()
@@ -620,18 +797,60 @@ def run_reference(args):
         step()
     dt = (time.perf_counter() - t) / args.steps
     v = xs.size / dt / 1e9
+    sample = (f"each step filters the first {sample_z} z-slices {list(xs.shape)} of the stack "
+              f"(all five filters), {threads} host threads")
     return {
         "metric": METRIC, "value": v, "unit": "Gvox/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic", "impl": "reference",
-        "config": {"workload": "3-D uint16 stack: gaussian(1,2,2) mirror->f32, sobel x3 ->f32, "
-                               "uniform(5)->u16", "shape": list(shape),
-                   "sample": f"{xs.shape} z-slab per step"},
+        "config": stack_config(shape, world), "sample": sample,
         "cpu_baseline": {"value": v, "unit": "Gvox/s", "cores": threads, "kind": "port",
-                         "sample": f"{xs.shape} z-slab of the stack per step"},
+                         "sample": sample},
         "e2e": {"value": v, "unit": "Gvox/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+
+
+def per_config_records(res, roof, cpu, peaks):
+    """One record per workload: its throughput, roofline, CPU baseline (the
+    oracle with all host threads) and parity, side by side."""
+    out = {"stack_512x1024x1024_u16": {
+        "value": res["value"], "unit": "Gvox/s", "roofline": roof, "cpu_baseline": cpu,
+        "parity": (res["parity"] or {}).get("bit_exact")}}
+    p2 = res["plain2d"]
+    if p2:
+        out["gaussian_2048x2048_f32_sigma4"] = {
+            "value": p2["gpx_s"], "unit": "Gpx/s",
+            "roofline": {"bound": "hbm", "achieved": p2["gb_s"], "peak": peaks.get("hbm_gbs"),
+                         "unit": "GB/s", "frac": p2.get("frac_of_hbm")},
+            "cpu_baseline": p2.get("cpu_baseline"), "parity": p2.get("oracle_bit_exact")}
+    pr = res["precision"]
+    if pr:
+        for name, row in pr["filters"].items():
+            t = row["tensor_tf32x3"]
+            out[f"precision_8192x8192_f32 {name}"] = {
+                "value": t["gpx_s"], "unit": "Gpx/s", "plain_f32_gpx_s": row["plain_f32"]["gpx_s"],
+                "speedup_vs_plain_f32": row["speedup"],
+                "max_rel_err": t["max_rel_err"], "plain_max_rel_err": row["plain_f32"]["max_rel_err"],
+                "roofline": {"bound": "tensor", "achieved": t["executed_tflops"],
+                             "peak": pr["tf32_peak_tflops"], "unit": "TFLOP/s",
+                             "frac": t.get("frac_of_tf32_peak")},
+                "cpu_baseline": pr.get("cpu_baseline")}
+    tl = res["tiles"]
+    if tl:
+        out["batched_tiles_4096_rgb_u8"] = {
+            "value": tl["batched_gpx_s"], "unit": "Gpx/s", "speedup_vs_per_tile": tl["speedup"],
+            "roofline": {"bound": "hbm", "achieved": 7 * tl["batched_gpx_s"],
+                         "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
+                         "frac": 7 * tl["batched_gpx_s"] / peaks["hbm_gbs"]
+                         if peaks.get("hbm_gbs") else None},
+            "cpu_baseline": tl.get("cpu_baseline"), "parity": tl.get("oracle_bit_exact")}
+    fr = res["frangi"]
+    if fr:
+        out["frangi_256cube_sigmas1to5"] = {
+            "value": fr["plain_f32"]["gvox_s"], "unit": "Gvox/s",
+            "cpu_baseline": fr.get("cpu_baseline"), "parity": fr.get("oracle")}
+    return out
 
 
 def _peaks():
@@ -646,7 +865,7 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
     if args.impl == "reference":
         if rank == 0:
-            print(json.dumps(run_reference(args)))
+            print(json.dumps(run_reference(args, world)))
         return
     import torch
     import torch.distributed as dist
@@ -697,13 +916,12 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["ms"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
-            "config": {"workload": "3-D uint16 stack: gaussian(1,2,2) mirror->f32, sobel x3 ->f32, "
-                                   "uniform(5)->u16 (bit-exact)", "shape": list(res["x"].shape),
-                       "voxels_per_step": res["nvox"], "l2": "inputs 1 GiB > L2, no flush",
-                       "parallelism": f"replicas x{world}"},
+            "config": stack_config(tuple(res["x"].shape), world),
             "roofline": roof, "kernels": res["kernels"], "cpu_baseline": cpu,
             "e2e": res["e2e"], "gpu_launches": LAUNCHES_PER_STEP * args.steps,
-            "clocks": res["clocks"], "precision_path": res["precision"],
+            "clocks": res["clocks"], "parity": res["parity"],
+            "per_config": per_config_records(res, roof, cpu, peaks),
+            "precision_path": res["precision"],
             "batched_tiles": res["tiles"], "frangi": res["frangi"],
             "plain_2d_gaussian": res["plain2d"],
         }

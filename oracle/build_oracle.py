@@ -27,7 +27,7 @@ def build(force=False):
         return OUT
     cmd = [
         "gcc",
-        "-O2",
+        "-O3",
         "-fPIC",
         "-shared",
         "-ffp-contract=off",

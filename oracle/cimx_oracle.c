@@ -237,14 +237,154 @@ double oracle_cval_as_input(double cval, int dt, int w64) {
  * already reversed for a convolution); anchor = K/2 + origin; cval_w is the
  * fill value as a W value. threads > 1 splits the lines with OpenMP.
  */
+/* n elements of `in` starting at index e, converted as load_f() converts
+ * them, into dst (the common input types get a plain loop). */
+static inline void load_row_f(const void* in, int tin, int64_t e, int64_t n, float* dst) {
+  if (tin == 'f') {
+    const float* s = (const float*)in + e;
+    for (int64_t i = 0; i < n; ++i) dst[i] = s[i];
+  } else if (tin == 'H') {
+    const uint16_t* s = (const uint16_t*)in + e;
+    for (int64_t i = 0; i < n; ++i) dst[i] = (float)s[i];
+  } else if (tin == 'B') {
+    const uint8_t* s = (const uint8_t*)in + e;
+    for (int64_t i = 0; i < n; ++i) dst[i] = (float)s[i];
+  } else {
+    for (int64_t i = 0; i < n; ++i) dst[i] = load_f(in, tin, e + i);
+  }
+}
+
+/* store_cast() of n float32 sums to consecutive elements from index e. */
+static inline void store_row_f(void* out, int tout, int64_t e, int64_t n, const float* acc) {
+  if (tout == 'f') {
+    float* d = (float*)out + e;
+    for (int64_t i = 0; i < n; ++i) d[i] = acc[i];
+  } else {
+    for (int64_t i = 0; i < n; ++i) store_cast(out, tout, e + i, (double)acc[i], 0);
+  }
+}
+
+/* The float32 chain of oracle_correlate1d, organised for speed: the same
+ * k-ascending fmaf() chain per output, with the boundary map evaluated once
+ * per (border output, tap) instead of per element. A pass along the last
+ * axis converts each line to float32 once and advances the chains of up to
+ * ORACLE_LINE_BLOCK consecutive outputs together; a pass along another axis
+ * runs over blocks of adjacent lines so that each tap reads a contiguous
+ * row. The chains of different outputs are independent, so interleaving
+ * them changes no result. Built twice (x86-64-v3 and baseline) and chosen
+ * at load time: the hardware FMA of the first clone rounds exactly like
+ * fmaf(). */
+#define ORACLE_LINE_BLOCK 64
+__attribute__((target_clones("arch=x86-64-v3", "default")))
+static void corr_f32(const void* in, int tin, void* out, int tout, int64_t outer, int64_t L,
+                     int64_t inner, const float* wf, int K, int anchor, float cval_f,
+                     int skip_zero, int threads, const int64_t* bmap, int64_t lo_int,
+                     int64_t hi_int) {
+  /* bmap[(l < lo_int ? l : lo_int + l - hi_int) * K + k]: the mapped index
+   * of tap k for the border outputs l < lo_int and l >= hi_int */
+  const int64_t nblk = inner == 1 ? 1 : (inner + ORACLE_LINE_BLOCK - 1) / ORACLE_LINE_BLOCK;
+  const int64_t nwork = outer * nblk;
+#if defined(_OPENMP)
+#pragma omp parallel num_threads(threads > 0 ? threads : 1)
+#else
+  (void)threads;
+#endif
+  {
+    float* line = inner == 1 ? (float*)malloc(sizeof(float) * (size_t)(L > 0 ? L : 1)) : 0;
+#if defined(_OPENMP)
+#pragma omp for schedule(dynamic, 1)
+#endif
+    for (int64_t wkey = 0; wkey < nwork; ++wkey) {
+      float acc[ORACLE_LINE_BLOCK];
+      float row[ORACLE_LINE_BLOCK];
+      if (inner == 1) {
+        if (!line) continue;
+        const int64_t base = wkey * L;
+        load_row_f(in, tin, base, L, line);
+        for (int64_t l0 = lo_int; l0 < hi_int; l0 += ORACLE_LINE_BLOCK) {
+          const int64_t n = hi_int - l0 < ORACLE_LINE_BLOCK ? hi_int - l0 : ORACLE_LINE_BLOCK;
+          for (int64_t j = 0; j < n; ++j) acc[j] = 0.0f;
+          for (int k = 0; k < K; ++k) {
+            const float w = wf[k];
+            if (skip_zero && w == 0.0f) continue;
+            const float* src = line + l0 - anchor + k;
+            for (int64_t j = 0; j < n; ++j) acc[j] = fmaf(src[j], w, acc[j]);
+          }
+          store_row_f(out, tout, base + l0, n, acc);
+        }
+        for (int64_t l = 0; l < L; ++l) {
+          if (l >= lo_int && l < hi_int) continue;
+          const int64_t* bm = bmap + (l < lo_int ? l : lo_int + l - hi_int) * K;
+          float s = 0.0f;
+          for (int k = 0; k < K; ++k) {
+            const float w = wf[k];
+            if (skip_zero && w == 0.0f) continue;
+            s = fmaf(bm[k] < 0 ? cval_f : line[bm[k]], w, s);
+          }
+          store_row_f(out, tout, base + l, 1, &s);
+        }
+        continue;
+      }
+      const int64_t o = wkey / nblk, i0 = (wkey % nblk) * ORACLE_LINE_BLOCK;
+      const int64_t nb = inner - i0 < ORACLE_LINE_BLOCK ? inner - i0 : ORACLE_LINE_BLOCK;
+      const int64_t base = o * L * inner + i0;
+      for (int64_t l = 0; l < L; ++l) {
+        for (int64_t i = 0; i < nb; ++i) acc[i] = 0.0f;
+        const int border = l < lo_int || l >= hi_int;
+        const int64_t* bm = border ? bmap + (l < lo_int ? l : lo_int + l - hi_int) * K : 0;
+        for (int k = 0; k < K; ++k) {
+          const float w = wf[k];
+          if (skip_zero && w == 0.0f) continue;
+          const int64_t ix = border ? bm[k] : l - anchor + k;
+          const float* src;
+          if (ix < 0) {
+            for (int64_t i = 0; i < nb; ++i) row[i] = cval_f;
+            src = row;
+          } else if (tin == 'f') {
+            src = (const float*)in + base + ix * inner;
+          } else {
+            load_row_f(in, tin, base + ix * inner, nb, row);
+            src = row;
+          }
+          for (int64_t i = 0; i < nb; ++i) acc[i] = fmaf(src[i], w, acc[i]);
+        }
+        store_row_f(out, tout, base + l * inner, nb, acc);
+      }
+    }
+    free(line);
+  }
+}
+
 void oracle_correlate1d(const void* in, int tin, void* out, int tout, int64_t outer,
                         int64_t L, int64_t inner, const double* taps, int K, int anchor,
                         int mode, double cval_w, int w64, int skip_zero, int threads) {
   const int64_t nlines = outer * inner;
-  /* float32 copies of the taps, any K (heap: tap counts reach the thousands) */
-  float* wf = (float*)malloc(sizeof(float) * (size_t)(K > 0 ? K : 1));
-  if (!wf) return;
-  for (int k = 0; k < K; ++k) wf[k] = (float)taps[k];
+  if (!w64) {
+    /* float32 copies of the taps, any K (heap: tap counts reach the thousands) */
+    float* wf = (float*)malloc(sizeof(float) * (size_t)(K > 0 ? K : 1));
+    if (!wf) return;
+    for (int k = 0; k < K; ++k) wf[k] = (float)taps[k];
+    /* outputs l in [lo_int, hi_int) read only in-range inputs */
+    int64_t lo_int = anchor < L ? anchor : L;
+    int64_t hi_int = L - (K - 1 - anchor);
+    if (hi_int < lo_int) hi_int = lo_int;
+    const int64_t nborder = lo_int + (L - hi_int);
+    int64_t* bmap = (int64_t*)malloc(sizeof(int64_t) * (size_t)(nborder * K > 0 ? nborder * K : 1));
+    if (!bmap) {
+      free(wf);
+      return;
+    }
+    for (int64_t l = 0; l < L; ++l) {
+      if (l >= lo_int && l < hi_int) continue;
+      int64_t* bm = bmap + (l < lo_int ? l : lo_int + l - hi_int) * K;
+      for (int k = 0; k < K; ++k) bm[k] = map_index(l - anchor + k, L, mode);
+    }
+    corr_f32(in, tin, out, tout, outer, L, inner, wf, K, anchor, (float)cval_w, skip_zero,
+             threads, bmap, lo_int, hi_int);
+    free(bmap);
+    free(wf);
+    return;
+  }
 #if defined(_OPENMP)
 #pragma omp parallel for schedule(static) num_threads(threads > 0 ? threads : 1)
 #else
@@ -254,38 +394,25 @@ void oracle_correlate1d(const void* in, int tin, void* out, int tout, int64_t ou
     const int64_t o = line / inner, i = line % inner;
     const int64_t base = o * L * inner + i;
     for (int64_t l = 0; l < L; ++l) {
-      if (w64) {
-        double s = 0.0;
-        for (int k = 0; k < K; ++k) {
-          const double w = taps[k];
-          if (skip_zero && w == 0.0) continue;
-          const int64_t ix = map_index(l - anchor + k, L, mode);
-          double x;
-          if (ix < 0) {
-            x = cval_w;
-          } else {
-            const int64_t e = base + ix * inner;
-            if (tin == 'L' || tin == 'Q') x = (double)((const uint64_t*)in)[e];
-            else if (tin == 'l' || tin == 'q') x = (double)((const int64_t*)in)[e];
-            else x = load_d(in, tin, e);
-          }
-          s = fma(x, w, s);
+      double s = 0.0;
+      for (int k = 0; k < K; ++k) {
+        const double w = taps[k];
+        if (skip_zero && w == 0.0) continue;
+        const int64_t ix = map_index(l - anchor + k, L, mode);
+        double x;
+        if (ix < 0) {
+          x = cval_w;
+        } else {
+          const int64_t e = base + ix * inner;
+          if (tin == 'L' || tin == 'Q') x = (double)((const uint64_t*)in)[e];
+          else if (tin == 'l' || tin == 'q') x = (double)((const int64_t*)in)[e];
+          else x = load_d(in, tin, e);
         }
-        store_cast(out, tout, base + l * inner, s, 1);
-      } else {
-        float s = 0.0f;
-        for (int k = 0; k < K; ++k) {
-          const float w = wf[k];
-          if (skip_zero && w == 0.0f) continue;
-          const int64_t ix = map_index(l - anchor + k, L, mode);
-          const float x = ix < 0 ? (float)cval_w : load_f(in, tin, base + ix * inner);
-          s = fmaf(x, w, s);
-        }
-        store_cast(out, tout, base + l * inner, (double)s, 0);
+        s = fma(x, w, s);
       }
+      store_cast(out, tout, base + l * inner, s, 1);
     }
   }
-  free(wf);
 }
 
 /* Elementwise cast of a W-typed array (float32 when w64 == 0) into dtype dt

@@ -291,6 +291,9 @@ def correlate1d(input, weights, axis=-1, output=None, mode="reflect", cval=0.0,
             and not np.isfinite(cval):
         raise NotImplementedError(
             "Non-finite cval is not supported for outputs with integer dtype.")
+    if out.flags.c_contiguous and not np.shares_memory(out, input):
+        _run_pass(input, out, axis, *params[:-1])  # straight into the output
+        return out
     res = np.empty(input.shape, out.dtype)
     _run_pass(input, res, axis, *params[:-1])
     out[...] = res
@@ -319,11 +322,14 @@ def run_1d_correlates(input, axes, weight_list, output, modes, cval, origins=0,
         output[...] = input
         return output
     cur = input
-    for ax, w, m, o in work:
-        res = np.empty(input.shape, output.dtype)
+    direct = output.flags.c_contiguous and not np.shares_memory(output, input)
+    for i, (ax, w, m, o) in enumerate(work):
+        last = i == len(work) - 1
+        res = output if (last and direct) else np.empty(input.shape, output.dtype)
         correlate1d(cur, w, ax, res, m, cval, o, algorithm=algorithm, convolve=convolve)
         cur = res
-    output[...] = cur
+    if cur is not output:
+        output[...] = cur
     return output
 
 
@@ -813,9 +819,55 @@ def eigvals_sym(elems, sort="descending", abs_sort=False):
         return np.stack(lam)
 
 
+def _by_chunks(fn, arrays):
+    """fn(*chunks) over chunks of the inputs' leading axis, in THREADS threads
+    (numpy releases the GIL in its loops). fn must be elementwise; its
+    results may carry extra leading axes (a stack of eigenvalue images), so
+    the chunks are joined along the axis that was the inputs' leading one.
+    The result equals fn(*arrays)."""
+    n = arrays[0].shape[0]
+    nchunk = max(1, min(THREADS, n))
+    if nchunk == 1:
+        return fn(*arrays)
+    from concurrent.futures import ThreadPoolExecutor
+
+    bounds = [(i * n // nchunk, (i + 1) * n // nchunk) for i in range(nchunk)]
+    with ThreadPoolExecutor(nchunk) as ex:
+        parts = list(ex.map(lambda b: fn(*[a[b[0]:b[1]] for a in arrays]), bounds))
+    nd = arrays[0].ndim
+    return np.concatenate(parts, axis=parts[0].ndim - nd)
+
+
+def _frangi_rg(ev, F):
+    rg = np.zeros(ev.shape[1:], F)
+    for lam in ev:
+        rg = (rg + lam.astype(np.float64) * lam).astype(F)
+    return rg
+
+
+def _frangi_scale(ev, rg, F, alpha_sq, beta_sq, gamma_sq):
+    if ev.shape[0] == 2:
+        l1, l2 = ev
+        rb = (np.abs(l1) / np.maximum(l2, F.type(1e-10))).astype(F)
+        rb = (rb * rb).astype(F)
+        v = np.exp(-rb.astype(np.float64) / beta_sq).astype(F)
+        return (v * (1.0 - np.exp(-rg.astype(np.float64) / gamma_sq))).astype(F)
+    l1, l2, l3 = ev
+    lam2 = np.maximum(l2, F.type(1e-10))
+    lam3 = np.maximum(l3, F.type(1e-10))
+    ra = (lam2 / lam3).astype(F)
+    ra = (ra * ra).astype(F)
+    rb = ((l1 * l1).astype(F) / (lam2 * lam3).astype(F)).astype(F)
+    v = (1.0 - np.exp(-ra.astype(np.float64) / alpha_sq)).astype(F)
+    v = (v * np.exp(-rb.astype(np.float64) / beta_sq)).astype(F)
+    return (v * (1.0 - np.exp(-rg.astype(np.float64) / gamma_sq))).astype(F)
+
+
 def frangi(image, sigmas=range(1, 10, 2), alpha=0.5, beta=0.5, gamma=None,
            black_ridges=True, mode="reflect", cval=0):
-    """filters/ridges.py:322-476 with the kernels of :228-319."""
+    """filters/ridges.py:322-476 with the kernels of :228-319. The eigenvalue
+    and vesselness steps are elementwise and run over chunks of the leading
+    axis in THREADS threads."""
     image = np.asarray(image)
     image = image.astype(supported_float_type(image.dtype), copy=False)
     if not black_ridges:
@@ -826,30 +878,15 @@ def frangi(image, sigmas=range(1, 10, 2), alpha=0.5, beta=0.5, gamma=None,
     fmax = None
     for sigma in sigmas:
         H = hessian_matrix_gaussian(image, sigma, mode=mode, cval=cval)
-        ev = eigvals_sym(H, sort="ascending", abs_sort=True)
-        rg = np.zeros(image.shape, F)
-        for lam in ev:
-            rg = (rg + lam.astype(np.float64) * lam).astype(F)
+        ev = _by_chunks(lambda *h: eigvals_sym(list(h), sort="ascending", abs_sort=True), H)
+        del H
+        rg = _by_chunks(lambda *e: _frangi_rg(np.stack(e), F), list(ev))
         if gamma_sq is None:
             s_max = float(rg.max())
             g = math.sqrt(s_max) / 2.0
             gamma_sq = 2.0 if s_max == 0 else max(2 * g * g, 1e-10)
-        if image.ndim == 2:
-            l1, l2 = ev
-            rb = (np.abs(l1) / np.maximum(l2, F.type(1e-10))).astype(F)
-            rb = (rb * rb).astype(F)
-            v = np.exp(-rb.astype(np.float64) / beta_sq).astype(F)
-            v = (v * (1.0 - np.exp(-rg.astype(np.float64) / gamma_sq))).astype(F)
-        else:
-            l1, l2, l3 = ev
-            lam2 = np.maximum(l2, F.type(1e-10))
-            lam3 = np.maximum(l3, F.type(1e-10))
-            ra = (lam2 / lam3).astype(F)
-            ra = (ra * ra).astype(F)
-            rb = ((l1 * l1).astype(F) / (lam2 * lam3).astype(F)).astype(F)
-            v = (1.0 - np.exp(-ra.astype(np.float64) / alpha_sq)).astype(F)
-            v = (v * np.exp(-rb.astype(np.float64) / beta_sq)).astype(F)
-            v = (v * (1.0 - np.exp(-rg.astype(np.float64) / gamma_sq))).astype(F)
+        v = _by_chunks(lambda r, *e: _frangi_scale(np.stack(e), r, F, alpha_sq, beta_sq,
+                                                   gamma_sq), [rg] + list(ev))
         fmax = v.copy() if fmax is None else np.maximum(fmax, v)
     return fmax
 
