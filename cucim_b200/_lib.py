@@ -129,6 +129,55 @@ _sigs = {
          _P(ctypes.c_float), _P(ctypes.c_float), ctypes.c_void_p],
         ctypes.c_int,
     ),
+    "cimx_gaussian_taps": (
+        [ctypes.c_double, ctypes.c_int, ctypes.c_int, _P(ctypes.c_double)], ctypes.c_int,
+    ),
+    "cimx_gaussian_nd": (
+        [_A, _A, _P(ctypes.c_double), _P(ctypes.c_int), _P(ctypes.c_int), _P(ctypes.c_int),
+         _P(ctypes.c_int), ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+         ctypes.c_int, ctypes.c_void_p],
+        ctypes.c_int,
+    ),
+    "cimx_uniform_nd": (
+        [_A, _A, _P(ctypes.c_int), _P(ctypes.c_int), _P(ctypes.c_int), _P(ctypes.c_int),
+         ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_void_p],
+        ctypes.c_int,
+    ),
+    "cimx_sobel_nd": (
+        [_A, _A, ctypes.c_int, _P(ctypes.c_int), ctypes.c_double, ctypes.c_int, ctypes.c_int,
+         ctypes.c_int, ctypes.c_void_p],
+        ctypes.c_int,
+    ),
+    "cimx_gaussian_gradient_magnitude_nd": (
+        [_A, _A, _P(ctypes.c_double), _P(ctypes.c_int), ctypes.c_double, ctypes.c_double,
+         ctypes.c_int, ctypes.c_void_p],
+        ctypes.c_int,
+    ),
+    "cimx_hessian": (
+        [_A, _A, ctypes.c_int, _P(ctypes.c_double), ctypes.c_int, ctypes.c_double, ctypes.c_int,
+         ctypes.c_int, ctypes.c_int, ctypes.c_void_p],
+        ctypes.c_int,
+    ),
+    "cimx_frangi": (
+        [_A, _A, _P(ctypes.c_double), ctypes.c_int, ctypes.c_double, ctypes.c_double,
+         ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int,
+         ctypes.c_void_p],
+        ctypes.c_int,
+    ),
+    "cimx_meijering_accumulate": (
+        [_A, ctypes.c_int, _A, ctypes.c_double, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p],
+        ctypes.c_int,
+    ),
+    "cimx_sato_accumulate": (
+        [_A, ctypes.c_int, _A, ctypes.c_double, ctypes.c_int, ctypes.c_void_p], ctypes.c_int,
+    ),
+    "cimx_nonpositive_to_one": ([_A, ctypes.c_void_p], ctypes.c_int),
+    "cimx_ridge_filter": (
+        [_A, _A, ctypes.c_int, _P(ctypes.c_double), ctypes.c_int, ctypes.c_double,
+         ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+         ctypes.c_int, ctypes.c_void_p],
+        ctypes.c_int,
+    ),
     "cimx_frangi_accumulate": (
         [_A, ctypes.c_int, _A, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int,
          ctypes.c_void_p, ctypes.c_void_p],

@@ -1,6 +1,7 @@
-"""gaussian, sobel, prewitt and frangi of cucim.skimage.filters
-(python/cucim/src/cucim/skimage/_shared/filters.py:21-166,
-filters/edges.py:148-330 and :494, filters/ridges.py:228-476)."""
+"""gaussian, sobel, prewitt and the ridge filters (frangi, meijering, sato,
+hessian) of cucim.skimage.filters (python/cucim/src/cucim/skimage/
+_shared/filters.py:21-166, filters/edges.py:148-330 and :494,
+filters/ridges.py:50-595)."""
 
 import ctypes
 import math
@@ -15,7 +16,8 @@ from .._util import check_mode, supported_float_type
 from . import util as _u
 from .feature import _hessian_matrix_with_gaussian, symmetric_compute_eigenvalues
 
-__all__ = ["gaussian", "difference_of_gaussians", "unsharp_mask", "sobel", "prewitt", "frangi"]
+__all__ = ["gaussian", "difference_of_gaussians", "unsharp_mask", "sobel", "prewitt", "frangi",
+           "meijering", "sato", "hessian"]
 
 
 def gaussian(image, sigma=1, mode="nearest", cval=0, preserve_range=False, truncate=4.0, *,
@@ -219,3 +221,75 @@ def frangi(image, sigmas=range(1, 10, 2), scale_range=None, scale_step=None, alp
                                              _arrays.stream_of(out))
         _lib.check(rc, "frangi")
     return _arrays.wrap_like(image, out)
+
+
+def _ridge_image(image, black_ridges, names):
+    """image.astype(_supported_float_type), negated for white ridges
+    (ridges.py:107-109, :200-202)."""
+    x = _arrays.as_tensor(image)
+    if x.dim() not in (2, 3):
+        raise NotImplementedError(
+            f"{names} is implemented here for 2-D and 3-D images (the closed-form eigenvalues)")
+    fdt = supported_float_type(_arrays.np_dtype(x))
+    img = _u.astype(image, fdt) if black_ridges else _u.negative_astype(image, fdt)
+    return img, x.dim(), fdt, x.shape, x.device
+
+
+def _eig_arrays(H, ndim):
+    ev = _arrays.as_tensor(symmetric_compute_eigenvalues(H))  # descending
+    return ev, (_lib.CimxArray * ndim)(*[_arrays.to_cimx(ev[k]) for k in range(ndim)])
+
+
+def meijering(image, sigmas=range(1, 10, 2), alpha=None, black_ridges=True, mode="reflect",
+              cval=0):
+    """ridges.py:50-146: Meijering neuriteness. Per scale the eigenvalues of
+    the Gaussian-derivative Hessian (descending) are mixed by the circulant
+    matrix (1 on the diagonal, alpha = 1 / (ndim + 1) by default elsewhere),
+    the mixed value of largest magnitude is kept, clipped at 0, normalised by
+    its maximum over the image (reduced on the device: no host
+    synchronisation) and folded into the maximum over scales."""
+    img, ndim, fdt, shape, device = _ridge_image(image, black_ridges, "meijering")
+    if alpha is None:
+        alpha = 1 / (ndim + 1)
+    out = torch.zeros(tuple(shape), dtype=_arrays.torch_dtype(fdt), device=device)
+    state = torch.zeros(2, dtype=torch.int64, device=device)
+    a_out = _arrays.to_cimx(out)
+    for i, sigma in enumerate(sigmas):
+        H = _hessian_matrix_with_gaussian(img, sigma, mode=mode, cval=cval)
+        ev, eigs = _eig_arrays(H, ndim)
+        rc = _lib.lib.cimx_meijering_accumulate(eigs, ndim, ctypes.byref(a_out), float(alpha),
+                                                1 if i == 0 else 0,
+                                                ctypes.c_void_p(state.data_ptr()),
+                                                _arrays.stream_of(out))
+        _lib.check(rc, "meijering")
+    return _arrays.wrap_like(img, out)
+
+
+def sato(image, sigmas=range(1, 10, 2), black_ridges=True, mode="reflect", cval=0):
+    """ridges.py:148-225: Sato tubeness. Per scale the geometric mean of the
+    Hessian eigenvalues but the lowest, clipped at 0, times sigma^2, folded
+    into the maximum over scales."""
+    img, ndim, fdt, shape, device = _ridge_image(image, black_ridges, "sato")
+    out = torch.zeros(tuple(shape), dtype=_arrays.torch_dtype(fdt), device=device)
+    a_out = _arrays.to_cimx(out)
+    for i, sigma in enumerate(sigmas):
+        H = _hessian_matrix_with_gaussian(img, sigma, mode=mode, cval=cval)
+        ev, eigs = _eig_arrays(H, ndim)
+        rc = _lib.lib.cimx_sato_accumulate(eigs, ndim, ctypes.byref(a_out), float(sigma),
+                                           1 if i == 0 else 0, _arrays.stream_of(out))
+        _lib.check(rc, "sato")
+    return _arrays.wrap_like(img, out)
+
+
+def hessian(image, sigmas=range(1, 10, 2), scale_range=None, scale_step=None, alpha=0.5,
+            beta=0.5, gamma=15, black_ridges=True, mode="reflect", cval=0):
+    """ridges.py:479-595: the hybrid Hessian filter, frangi with gamma 15 by
+    default and every output <= 0 set to 1."""
+    out = frangi(image, sigmas=sigmas, scale_range=scale_range, scale_step=scale_step,
+                 alpha=alpha, beta=beta, gamma=gamma, black_ridges=black_ridges, mode=mode,
+                 cval=cval)
+    t = _arrays.as_tensor(out)
+    a = _arrays.to_cimx(t)
+    _lib.check(_lib.lib.cimx_nonpositive_to_one(ctypes.byref(a), _arrays.stream_of(t)),
+               "hessian")
+    return out

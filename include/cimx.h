@@ -269,6 +269,134 @@ CIMX_API int cimx_frangi_accumulate(const CimxArray* eigs, int ndim, const CimxA
                                     double alpha, double beta, double gamma, int first,
                                     void* gamma_state, void* stream);
 
+/* ---------------------------------------------------------------------
+ * Whole filters in one call, for hosts without the Python layer. Each entry
+ * restates cuCIM's host-side rules in C++ (per-axis arguments, sigma and
+ * radius cut-offs, tap generation, the weights type, the choice between
+ * cuCIM's shared-memory and elementwise kernels) and runs the same kernels
+ * as the Python package. Modes are CIMX_MODE_* codes ('wrap' passed as
+ * CIMX_MODE_GRID_WRAP); `algorithm` is cuCIM's algorithm= keyword.
+ * --------------------------------------------------------------------- */
+enum {
+  CIMX_ALGO_AUTO = 0,           /* algorithm=None */
+  CIMX_ALGO_SHARED_MEMORY = 1,  /* algorithm='shared_memory' */
+  CIMX_ALGO_ELEMENTWISE = 2,    /* algorithm='elementwise' */
+};
+
+/* The float64 correlation taps of a Gaussian (derivative) of `order` with
+ * 2 * radius + 1 taps, written to taps[0 .. 2 * radius]: cuCIM's
+ * _gaussian_kernel1d (_vendored/_ndimage_filters.py:689-717), with numpy's
+ * pairwise summation order for the normalisation and the C library's exp().
+ * numpy's own exp() differs from the C library's in the last bit for a few
+ * percent of arguments on hosts where numpy uses its AVX-512 code, so cuCIM's
+ * float64 taps themselves depend on the host. Over a sweep of sigmas
+ * (0.3-40, truncate 4, 8 and 100) the taps here are within 5 ulp of numpy's
+ * (orders 0 and 1; orders 2 and 3: 11 ulp of the largest tap, their
+ * polynomial cancelling near its roots), and bit for bit equal
+ * once rounded to float32, the weights type of float32 inputs and of every
+ * input of 16 bits or fewer; the test suite checks both. */
+CIMX_API int cimx_gaussian_taps(double sigma, int order, int radius, double* taps);
+
+/* gaussian_filter (_vendored/_ndimage_filters.py:580-686) over `naxes` axes
+ * (`axes` NULL: all axes, naxes == ndim), with per-axis sigma, order
+ * (NULL: 0), radius (NULL or a negative entry: int(truncate * sigma + 0.5))
+ * and mode. Axes with sigma <= 1e-15 or radius 0 are skipped; with none left
+ * the input is copied (cast) into the output. */
+CIMX_API int cimx_gaussian_nd(const CimxArray* in, const CimxArray* out, const double* sigma,
+                              const int* order, const int* radius, const int* modes,
+                              const int* axes, int naxes, double truncate, double cval,
+                              int algorithm, int lib_flags, void* stream);
+
+/* uniform_filter (_vendored/_ndimage_filters.py:447-521): per-axis size,
+ * mode and origin (NULL: 0) over `axes` (NULL: all); sizes of 1 skipped. */
+CIMX_API int cimx_uniform_nd(const CimxArray* in, const CimxArray* out, const int* sizes,
+                             const int* modes, const int* origins, const int* axes, int naxes,
+                             double cval, int algorithm, int lib_flags, void* stream);
+
+/* sobel (prewitt = 0) or prewitt (prewitt = 1) along `axis`
+ * (_vendored/_ndimage_filters.py:720-803): [-1, 0, 1] along `axis`, [1, 2, 1]
+ * or [1, 1, 1] along the other axes; `modes` holds one mode per axis. */
+CIMX_API int cimx_sobel_nd(const CimxArray* in, const CimxArray* out, int axis,
+                           const int* modes, double cval, int prewitt, int algorithm,
+                           int lib_flags, void* stream);
+
+/* gaussian_gradient_magnitude (_vendored/_ndimage_filters.py:1100-1157)
+ * with per-axis sigma; modes[a] is the mode of every pass of the derivative
+ * along axis a (generic_gradient_magnitude passes one mode per derivative);
+ * `out` float32 or float64. */
+CIMX_API int cimx_gaussian_gradient_magnitude_nd(const CimxArray* in, const CimxArray* out,
+                                                 const double* sigma, const int* modes,
+                                                 double truncate, double cval, int algorithm,
+                                                 void* stream);
+
+/* hessian_matrix (feature/corner.py:257-384): the ndim * (ndim + 1) / 2
+ * upper-triangular element images, in the order of
+ * combinations_with_replacement(axes, 2) (axes reversed when order_xy, 2-D
+ * only), written to elems[], each of the image's float type (float32 for
+ * inputs of 16 bits or fewer and float32, else float64). `sigma` holds one
+ * value per axis. use_gaussian_derivatives != 0: Gaussian-derivative
+ * filters at sigma / sqrt(2), truncate 8 (or 100 when some sigma <= 1)
+ * (corner.py:161-254); 0: skimage gaussian then numpy.gradient twice.
+ * Integer images are first converted as img_as_float does. Scratch: the
+ * converted image and ndim gradient images from the allocator. */
+CIMX_API int cimx_hessian(const CimxArray* in, const CimxArray* elems, int nelems,
+                          const double* sigma, int mode, double cval,
+                          int use_gaussian_derivatives, int order_xy, int lib_flags,
+                          void* stream);
+
+/* cimx_ridge_filter with CIMX_RIDGE_FRANGI: frangi vesselness
+ * (filters/ridges.py:322-476) of a 2-D or 3-D image over
+ * `nsigmas` scales: per scale the Gaussian-derivative Hessian, its
+ * eigenvalues sorted ascending by magnitude, and the vesselness folded into
+ * `out` (the image's float type) with a maximum. gamma = NaN selects the
+ * automatic gamma of the first scale, kept on the device (no host
+ * synchronisation). black_ridges = 0 negates the image first. Scratch: the
+ * image, the Hessian elements, their eigenvalues and the gradients. */
+CIMX_API int cimx_frangi(const CimxArray* in, const CimxArray* out, const double* sigmas,
+                         int nsigmas, double alpha, double beta, double gamma, int black_ridges,
+                         int mode, double cval, int lib_flags, void* stream);
+
+/* The ridge filters of filters/ridges.py over `nsigmas` scales, each built
+ * on the Gaussian-derivative Hessian and its closed-form eigenvalues, 2-D or
+ * 3-D images, `out` of the image's float type:
+ *   CIMX_RIDGE_FRANGI    frangi (:322-476), gamma NaN = automatic;
+ *   CIMX_RIDGE_MEIJERING meijering (:50-146), alpha NaN = 1 / (ndim + 1);
+ *   CIMX_RIDGE_SATO      sato (:148-225);
+ *   CIMX_RIDGE_HESSIAN   the hybrid hessian filter (:479-595): frangi with
+ *                        gamma NaN = 15, then outputs <= 0 set to 1.
+ * Arguments a filter does not use are ignored. Nothing synchronises the
+ * host: the automatic gamma and meijering's normalising maximum stay on the
+ * device. Scratch: the image, the Hessian elements, their eigenvalues and
+ * the gradients. */
+enum {
+  CIMX_RIDGE_FRANGI = 0,
+  CIMX_RIDGE_MEIJERING = 1,
+  CIMX_RIDGE_SATO = 2,
+  CIMX_RIDGE_HESSIAN = 3,
+};
+CIMX_API int cimx_ridge_filter(const CimxArray* in, const CimxArray* out, int kind,
+                               const double* sigmas, int nsigmas, double alpha, double beta,
+                               double gamma, int black_ridges, int mode, double cval,
+                               int lib_flags, void* stream);
+
+/* Per-scale epilogues of meijering and sato on the eigenvalue images of one
+ * scale (descending, as hessian_matrix_eigvals returns them), folded into
+ * `out` with a NaN-propagating maximum that starts from 0 (first != 0).
+ * meijering (filters/ridges.py:102-146): eigenvalues below 1e-12 in
+ * magnitude zeroed, mixed by the circulant matrix (1 on the diagonal, alpha
+ * elsewhere) as ascending multiply-add chains, the mixed value of largest
+ * magnitude clipped at 0 and divided by its maximum over the image, reduced
+ * into `state` (16 bytes of device memory owned by the caller) on the device.
+ * sato (:203-225): the geometric mean (powf) of the clipped eigenvalues but
+ * the lowest, times sigma^2. */
+CIMX_API int cimx_meijering_accumulate(const CimxArray* eigs, int ndim, const CimxArray* out,
+                                       double alpha, int first, void* state, void* stream);
+CIMX_API int cimx_sato_accumulate(const CimxArray* eigs, int ndim, const CimxArray* out,
+                                  double sigma, int first, void* stream);
+
+/* a[a <= 0] = 1 in place (the last step of filters/ridges.py:479-595). */
+CIMX_API int cimx_nonpositive_to_one(const CimxArray* a, void* stream);
+
 /* One tile of a batch for cimx_batch_gray_gauss_sobel. */
 typedef struct CimxBatchTile {
   const uint8_t* rgb;   /* device: height x width x 3 uint8, C-contiguous */

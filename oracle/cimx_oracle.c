@@ -443,3 +443,31 @@ void oracle_min_max1d(const void* in, int tin, void* out, int tout, int64_t oute
         store_cast(out, tout, base + l * inner, value, 1);
       }
 }
+
+/* rgb2gray's kernel body (color/colorconv.py:1038-1046),
+ *   gray = 0.2125 * r + 0.7154 * g + 0.0721 * b   (double),
+ * as the CUDA compiler evaluates it: cuCIM compiles it with NVRTC's default
+ * --fmad=true (CuPy passes no options), which contracts the first product
+ * into the first addition and the last product into the second:
+ * fma(0.0721, b, fma(0.2125, r, 0.7154 * g)). Checked against the GPU
+ * output of the same expression on 4.2 M float32 and uint8 pixels (no
+ * other association matched all of them). rgb holds n (r, g, b) triples
+ * already converted to double. */
+void oracle_rgb2gray(const double* rgb, int64_t n, double* out) {
+  for (int64_t i = 0; i < n; ++i) {
+    const double r = rgb[3 * i], g = rgb[3 * i + 1], b = rgb[3 * i + 2];
+    out[i] = fma(0.0721, b, fma(0.2125, r, 0.7154 * g));
+  }
+}
+
+/* out[i] = fma(a[i], b[i], c[i]) in float32 (w64 == 0) or float64, correctly
+ * rounded (libm): the multiply-add chains of cupy.tensordot's GEMM in
+ * meijering. */
+void oracle_fma(const void* a, const void* b, const void* c, int64_t n, int w64, void* out) {
+  for (int64_t i = 0; i < n; ++i) {
+    if (w64)
+      ((double*)out)[i] = fma(((const double*)a)[i], ((const double*)b)[i], ((const double*)c)[i]);
+    else
+      ((float*)out)[i] = fmaf(((const float*)a)[i], ((const float*)b)[i], ((const float*)c)[i]);
+  }
+}

@@ -41,6 +41,11 @@ _lib.oracle_min_max1d.argtypes = [
     ctypes.c_double, ctypes.c_int,
 ]
 _lib.oracle_min_max1d.restype = None
+_lib.oracle_rgb2gray.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p]
+_lib.oracle_rgb2gray.restype = None
+_lib.oracle_fma.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
+                            ctypes.c_int, ctypes.c_void_p]
+_lib.oracle_fma.restype = None
 
 MODES = {
     "reflect": 0, "grid-mirror": 0, "mirror": 1, "nearest": 2,
@@ -891,6 +896,85 @@ def frangi(image, sigmas=range(1, 10, 2), alpha=0.5, beta=0.5, gamma=None,
     return fmax
 
 
+def fma(a, b, c):
+    """Elementwise fused multiply-add in the arrays' float type (C core)."""
+    a, b, c = np.broadcast_arrays(*[np.asarray(v) for v in (a, b, c)])
+    F = np.result_type(a, b, c)
+    a, b, c = (np.ascontiguousarray(v, dtype=F) for v in (a, b, c))
+    out = np.empty(a.shape, F)
+    _lib.oracle_fma(a.ctypes.data, b.ctypes.data, c.ctypes.data, a.size,
+                    int(F == np.float64), out.ctypes.data)
+    return out
+
+
+def _ridge_image(image, black_ridges):
+    image = np.asarray(image)
+    image = image.astype(supported_float_type(image.dtype), copy=False)
+    return -image if not black_ridges else image
+
+
+def _ridge_eigvals(image, sigma, mode, cval):
+    """hessian_matrix_eigvals of the Gaussian-derivative Hessian (descending),
+    entries below 1e-12 in magnitude zeroed (ridges.py:112-116)."""
+    F = image.dtype
+    H = hessian_matrix_gaussian(image, sigma, mode=mode, cval=cval)
+    ev = _by_chunks(lambda *h: eigvals_sym(list(h), sort="descending"), H)
+    return np.where(np.abs(ev) < F.type(1e-12), F.type(0), ev).astype(F)
+
+
+def meijering(image, sigmas=range(1, 10, 2), alpha=None, black_ridges=True, mode="reflect",
+              cval=0):
+    """filters/ridges.py:50-146. The circulant mixing (cupy.tensordot, a
+    float GEMM over ndim products) is an ascending multiply-add chain."""
+    image = _ridge_image(image, black_ridges)
+    F = image.dtype
+    if alpha is None:
+        alpha = 1 / (image.ndim + 1)
+    a = F.type(alpha)
+    out = np.zeros_like(image)
+    for sigma in sigmas:
+        ev = _ridge_eigvals(image, sigma, mode, cval)
+        nd = ev.shape[0]
+        vals = []
+        for r in range(nd):
+            v = ((F.type(1) if r == 0 else a) * ev[0]).astype(F)
+            for k in range(1, nd):
+                v = fma(np.full(v.shape, F.type(1) if r == k else a, F), ev[k], v)
+            vals.append(v)
+        vals = np.stack(vals)
+        v = np.take_along_axis(vals, np.abs(vals).argmax(0)[None], 0)[0]
+        v = np.maximum(v, F.type(0))
+        mx = v.max()
+        if mx > 0:
+            v = (v / mx).astype(F)
+        out = np.maximum(out, v)
+    return out
+
+
+def sato(image, sigmas=range(1, 10, 2), black_ridges=True, mode="reflect", cval=0):
+    """filters/ridges.py:148-225."""
+    image = _ridge_image(image, black_ridges)
+    if image.ndim not in (2, 3):
+        raise ValueError("sato is defined for 2-D and 3-D images")
+    F = image.dtype
+    out = np.zeros_like(image)
+    for sigma in sigmas:
+        ev = _ridge_eigvals(image, sigma, mode, cval)[:-1]
+        vals = np.prod(np.maximum(ev, F.type(0)), 0).astype(F) ** F.type(1 / len(ev))
+        vals = (vals * F.type(sigma ** 2)).astype(F)
+        out = np.maximum(out, vals)
+    return out
+
+
+def hessian_ridge(image, sigmas=range(1, 10, 2), alpha=0.5, beta=0.5, gamma=15,
+                  black_ridges=True, mode="reflect", cval=0):
+    """filters/ridges.py:479-595: frangi, then outputs <= 0 set to 1."""
+    out = frangi(image, sigmas=sigmas, alpha=alpha, beta=beta, gamma=gamma,
+                 black_ridges=black_ridges, mode=mode, cval=cval)
+    out[out <= 0] = 1
+    return out
+
+
 def rgb2gray(rgb, channel_axis=-1):
     """color/colorconv.py:1049-1095 (+ _prepare_colorarray :160-183)."""
     rgb = np.moveaxis(np.asarray(rgb), channel_axis, -1)
@@ -899,7 +983,9 @@ def rgb2gray(rgb, channel_axis=-1):
     fdt = supported_float_type(rgb.dtype)
     x = img_as_float(rgb).astype(fdt)
     x = np.ascontiguousarray(x).astype(np.float64)
-    g = 0.2125 * x[..., 0] + 0.7154 * x[..., 1] + 0.0721 * x[..., 2]
+    g = np.empty(x.shape[:-1], np.float64)
+    # the kernel's expression with the CUDA compiler's contraction (C core)
+    _lib.oracle_rgb2gray(x.ctypes.data, g.size, g.ctypes.data)
     return g.astype(fdt)
 
 

@@ -314,17 +314,24 @@ def test_eigvals(ski, n, sort, abs_sort):
 
 @pytest.mark.parametrize("shape,black", [((40, 44), True), ((18, 20, 22), False)])
 def test_frangi(ski, shape, black):
+    """Bit-identical wherever the output is at least 1e-3 of its maximum,
+    within 1e-9 of the maximum elsewhere (see tests/test_gpu_ridges.py)."""
     x = _rand(shape, np.float32)
     got = host(ski.filters.frangi(dev(x), sigmas=[1, 2], black_ridges=black))
     exp = R.frangi(x, sigmas=[1, 2], black_ridges=black)
-    np.testing.assert_allclose(got, exp, rtol=1e-4, atol=1e-6)
+    big = np.abs(exp) >= 1e-3 * np.abs(exp).max()
+    np.testing.assert_array_equal(got[big], exp[big])
+    assert np.abs(got.astype(np.float64) - exp).max() <= 1e-9 * np.abs(exp).max()
 
 
-def test_rgb2gray(ski):
-    rgb = np.random.default_rng(0).integers(0, 256, (37, 41, 3)).astype(np.uint8)
+@pytest.mark.parametrize("dtype", [np.uint8, np.float32, np.float64])
+def test_rgb2gray(ski, dtype):
+    """Bit for bit: the oracle evaluates the kernel's expression with the
+    CUDA compiler's contraction (oracle/cimx_oracle.c)."""
+    rgb = np.random.default_rng(0).integers(0, 256, (257, 301, 3)).astype(np.uint8)
+    if dtype != np.uint8:
+        rgb = (rgb / 255 + np.random.default_rng(1).random(rgb.shape) * 1e-3).astype(dtype)
     got = host(ski.color.rgb2gray(dev(rgb)))
     exp = R.rgb2gray(rgb)
-    np.testing.assert_allclose(got, exp, rtol=1.2e-7, atol=0)
-    rgbf = rgb.astype(np.float32) / 255
-    np.testing.assert_allclose(host(ski.color.rgb2gray(dev(rgbf))), R.rgb2gray(rgbf),
-                               rtol=1.2e-7, atol=0)
+    assert got.dtype == exp.dtype
+    np.testing.assert_array_equal(got, exp)

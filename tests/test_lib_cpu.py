@@ -156,3 +156,58 @@ def test_wait_selftest_rejects_bad_arguments():
     assert _lib.lib.cimx_wait_selftest(0, 0, None) == _lib.E_INVALID
     assert _lib.lib.cimx_wait_selftest(0, 1 << 25, None) == _lib.E_INVALID
     assert _lib.lib.cimx_wait_selftest(1, 10 ** 9, None) == _lib.E_INVALID
+
+
+@pytest.mark.parametrize("order", [0, 1, 2, 3])
+def test_c_gaussian_taps_match_numpy(order):
+    """cimx_gaussian_taps (float64 taps generated in the library, for hosts
+    without numpy) against the numpy taps the Python layer uses: bit for bit
+    once rounded to float32, and within 5 ulp in float64 (orders 0-2; order 3
+    within 11 ulp of the largest tap): numpy's own exp() differs from the C
+    library's in the last bit on AVX-512 hosts."""
+    for s in list(np.linspace(0.3, 40, 61)) + [16.0, 32.0, 2 ** -0.5, 3 * 2 ** -0.5]:
+        for trunc in (4.0, 8.0, 100.0):
+            r = int(trunc * s + 0.5)
+            if r <= 0 or r > 2000:
+                continue
+            ref = ndi._gaussian_taps(float(s), order, r, np.float64)
+            got = np.empty(2 * r + 1)
+            rc = _lib.lib.cimx_gaussian_taps(float(s), order, r,
+                                             got.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+            assert rc == 0
+            np.testing.assert_array_equal(got.astype(np.float32), ref.astype(np.float32))
+            if order < 2:
+                ulps = np.abs(got - ref) / np.spacing(np.abs(ref))
+                assert ulps.max() <= 5, (s, r, ulps.max())
+            else:
+                assert (np.abs(got - ref) / np.spacing(np.abs(ref).max())).max() <= 11
+
+
+def test_c_entries_reject_bad_arguments():
+    a = _arr((6, 7), np.float32, 0x1000)
+    b = _arr((6, 7), np.float32, 0x9000)
+    sig = (ctypes.c_double * 2)(1.0, 1.0)
+    modes = (ctypes.c_int * 2)(0, 0)
+    axes = (ctypes.c_int * 2)(0, 0)
+    rc = _lib.lib.cimx_gaussian_nd(ctypes.byref(a), ctypes.byref(b), sig, None, None, modes,
+                                   axes, 2, 4.0, 0.0, 0, 0, None)
+    assert rc == _lib.E_INVALID and "unique" in _lib.last_error()
+    rc = _lib.lib.cimx_gaussian_nd(ctypes.byref(a), ctypes.byref(b), sig, None, None, modes,
+                                   None, 1, 4.0, 0.0, 0, 0, None)
+    assert rc == _lib.E_INVALID
+    bad_modes = (ctypes.c_int * 2)(0, 9)
+    rc = _lib.lib.cimx_sobel_nd(ctypes.byref(a), ctypes.byref(b), 0, bad_modes, 0.0, 0, 0, 0,
+                                None)
+    assert rc == _lib.E_INVALID and "mode" in _lib.last_error()
+    rc = _lib.lib.cimx_frangi(ctypes.byref(_arr((6,), np.float32, 0x1000)),
+                              ctypes.byref(_arr((6,), np.float32, 0x9000)), sig, 1, 0.5, 0.5,
+                              float("nan"), 1, 0, 0.0, 0, None)
+    assert rc == _lib.E_INVALID and "2-dimensional or 3-dimensional" in _lib.last_error()
+    u8 = _arr((6, 7), np.uint8, 0x9000)
+    rc = _lib.lib.cimx_gaussian_nd(ctypes.byref(a), ctypes.byref(u8), sig, None, None,
+                                   (ctypes.c_int * 2)(4, 4), None, 2, 4.0, float("nan"), 0, 0,
+                                   None)
+    assert rc == _lib.E_INVALID and "Non-finite cval" in _lib.last_error()
+    rc = _lib.lib.cimx_uniform_nd(ctypes.byref(a), ctypes.byref(b), (ctypes.c_int * 2)(3, 3),
+                                  modes, (ctypes.c_int * 2)(2, 0), None, 2, 0.0, 0, 0, None)
+    assert rc == _lib.E_INVALID and "origin" in _lib.last_error()
