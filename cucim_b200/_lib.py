@@ -172,6 +172,7 @@ _sigs = {
         [_A, ctypes.c_int, _A, ctypes.c_double, ctypes.c_int, ctypes.c_void_p], ctypes.c_int,
     ),
     "cimx_nonpositive_to_one": ([_A, ctypes.c_void_p], ctypes.c_int),
+    "cimx_mask_erode_multiply": ([_A, _A, ctypes.c_void_p], ctypes.c_int),
     "cimx_ridge_filter": (
         [_A, _A, ctypes.c_int, _P(ctypes.c_double), ctypes.c_int, ctypes.c_double,
          ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_double,

@@ -16,8 +16,9 @@ from .._util import check_mode, supported_float_type
 from . import util as _u
 from .feature import _hessian_matrix_with_gaussian, symmetric_compute_eigenvalues
 
-__all__ = ["gaussian", "difference_of_gaussians", "unsharp_mask", "sobel", "prewitt", "frangi",
-           "meijering", "sato", "hessian"]
+__all__ = ["gaussian", "difference_of_gaussians", "unsharp_mask", "sobel", "sobel_h", "sobel_v",
+           "scharr", "scharr_h", "scharr_v", "prewitt", "prewitt_h", "prewitt_v", "farid",
+           "farid_h", "farid_v", "frangi", "meijering", "sato", "hessian"]
 
 
 def gaussian(image, sigma=1, mode="nearest", cval=0, preserve_range=False, truncate=4.0, *,
@@ -50,6 +51,12 @@ def gaussian(image, sigma=1, mode="nearest", cval=0, preserve_range=False, trunc
 
 _SOBEL_SMOOTH = np.array([1, 2, 1]) / 4
 _PREWITT_SMOOTH = np.full((3,), 1 / 3)
+_SCHARR_SMOOTH = np.array([3, 10, 3]) / 16
+# Farid & Simoncelli's 5-tap filters (the coefficients of edges.py:60-70)
+_FARID_SMOOTH = np.array([0.0376593171958126, 0.249153396177344, 0.426374573253687,
+                          0.249153396177344, 0.0376593171958126])
+_FARID_EDGE = np.array([0.109603762960254, 0.276690988455557, 0, -0.276690988455557,
+                        -0.109603762960254])
 
 
 def difference_of_gaussians(image, low_sigma, high_sigma=None, *, mode="nearest", cval=0,
@@ -168,23 +175,100 @@ def _generic_edge_filter(image, *, smooth_weights, edge_weights=(1, 0, -1), axis
     return ndi._run(image, chains[0], fdt, 0.0)
 
 
-def _mask_unsupported(mask):
-    if mask is not None:
-        raise NotImplementedError("mask is not supported on this path")
+def _mask_filter_result(result, mask):
+    """edges.py:75-85: the mask eroded with the full-connectivity footprint
+    (border value 0) multiplies the result in place, on the device."""
+    if mask is None:
+        return result
+    t = _arrays.as_tensor(result)
+    m = _arrays.as_tensor(mask).contiguous()
+    if tuple(m.shape) != tuple(t.shape):
+        raise ValueError("mask must have the shape of the image")
+    a_r, a_m = _arrays.to_cimx(t), _arrays.to_cimx(m)
+    _lib.check(_lib.lib.cimx_mask_erode_multiply(ctypes.byref(a_r), ctypes.byref(a_m),
+                                                 _arrays.stream_of(t)), "mask")
+    return result
+
+
+def _check_2d(image):
+    if _arrays.as_tensor(image).dim() != 2:
+        raise ValueError("The parameter `image` must be a 2-dimensional array")
 
 
 def sobel(image, mask=None, *, axis=None, mode="reflect", cval=0.0):
-    """edges.py:244-306."""
-    _mask_unsupported(mask)
-    return _generic_edge_filter(image, smooth_weights=_SOBEL_SMOOTH, axis=axis, mode=mode,
-                                cval=cval)
+    """edges.py:244-299."""
+    out = _generic_edge_filter(image, smooth_weights=_SOBEL_SMOOTH, axis=axis, mode=mode,
+                               cval=cval)
+    return _mask_filter_result(out, mask)
+
+
+def sobel_h(image, mask=None):
+    """edges.py:302-329: horizontal edges of a 2-D image."""
+    _check_2d(image)
+    return sobel(image, mask=mask, axis=0)
+
+
+def sobel_v(image, mask=None):
+    """edges.py:332-359: vertical edges of a 2-D image."""
+    _check_2d(image)
+    return sobel(image, mask=mask, axis=1)
+
+
+def scharr(image, mask=None, *, axis=None, mode="reflect", cval=0.0):
+    """edges.py:362-422: smoothing taps [3, 10, 3] / 16."""
+    out = _generic_edge_filter(image, smooth_weights=_SCHARR_SMOOTH, axis=axis, mode=mode,
+                               cval=cval)
+    return _mask_filter_result(out, mask)
+
+
+def scharr_h(image, mask=None):
+    """edges.py:425-457."""
+    _check_2d(image)
+    return scharr(image, mask=mask, axis=0)
+
+
+def scharr_v(image, mask=None):
+    """edges.py:460-491."""
+    _check_2d(image)
+    return scharr(image, mask=mask, axis=1)
 
 
 def prewitt(image, mask=None, *, axis=None, mode="reflect", cval=0.0):
-    """edges.py:494-553."""
-    _mask_unsupported(mask)
-    return _generic_edge_filter(image, smooth_weights=_PREWITT_SMOOTH, axis=axis, mode=mode,
-                                cval=cval)
+    """edges.py:494-551."""
+    out = _generic_edge_filter(image, smooth_weights=_PREWITT_SMOOTH, axis=axis, mode=mode,
+                               cval=cval)
+    return _mask_filter_result(out, mask)
+
+
+def prewitt_h(image, mask=None):
+    """edges.py:554-581."""
+    _check_2d(image)
+    return prewitt(image, mask=mask, axis=0)
+
+
+def prewitt_v(image, mask=None):
+    """edges.py:584-611."""
+    _check_2d(image)
+    return prewitt(image, mask=mask, axis=1)
+
+
+def farid(image, mask=None, *, axis=None, mode="reflect", cval=0.0):
+    """edges.py:783-850: Farid's 5-tap derivative and smoothing filters."""
+    out = _generic_edge_filter(image, smooth_weights=_FARID_SMOOTH, edge_weights=_FARID_EDGE,
+                               axis=axis, mode=mode, cval=cval)
+    return _mask_filter_result(out, mask)
+
+
+def farid_h(image, *, mask=None):
+    """edges.py:853-890."""
+    _check_2d(image)
+    return farid(image, mask=mask, axis=0)
+
+
+def farid_v(image, *, mask=None):
+    """edges.py:893-927."""
+    _check_2d(image)
+    return farid(image, mask=mask, axis=1)
 
 
 def frangi(image, sigmas=range(1, 10, 2), scale_range=None, scale_step=None, alpha=0.5,

@@ -397,6 +397,14 @@ CIMX_API int cimx_sato_accumulate(const CimxArray* eigs, int ndim, const CimxArr
 /* a[a <= 0] = 1 in place (the last step of filters/ridges.py:479-595). */
 CIMX_API int cimx_nonpositive_to_one(const CimxArray* a, void* stream);
 
+/* The mask= argument of the skimage edge filters (filters/edges.py:75-85):
+ * `mask` (any real or bool dtype, nonzero = inside) is eroded with the
+ * full-connectivity footprint (the whole 3 x ... x 3 neighbourhood) with
+ * border value 0, and `result` (float32/float64, same shape, both
+ * C-contiguous) is multiplied by it in place. */
+CIMX_API int cimx_mask_erode_multiply(const CimxArray* result, const CimxArray* mask,
+                                      void* stream);
+
 /* One tile of a batch for cimx_batch_gray_gauss_sobel. */
 typedef struct CimxBatchTile {
   const uint8_t* rgb;   /* device: height x width x 3 uint8, C-contiguous */

@@ -669,6 +669,11 @@ def unsharp_mask(image, radius=1.0, amount=1.0, preserve_range=False, *, channel
 
 _SOBEL_SMOOTH = np.array([1, 2, 1]) / 4
 _PREWITT_SMOOTH = np.full((3,), 1 / 3)
+_SCHARR_SMOOTH = np.array([3, 10, 3]) / 16
+_FARID_SMOOTH = np.array([0.0376593171958126, 0.249153396177344, 0.426374573253687,
+                          0.249153396177344, 0.0376593171958126])
+_FARID_EDGE = np.array([0.109603762960254, 0.276690988455557, 0, -0.276690988455557,
+                        -0.109603762960254])
 
 
 def generic_edge_filter(image, *, smooth_weights, edge_weights=(1, 0, -1), axis=None,
@@ -706,12 +711,40 @@ def generic_edge_filter(image, *, smooth_weights, edge_weights=(1, 0, -1), axis=
     return output
 
 
+def mask_filter_result(result, mask):
+    """filters/edges.py:75-85: binary erosion of the mask with the
+    full-connectivity footprint and border value 0 (scipy.ndimage's
+    binary_erosion, the same definition), then result *= mask."""
+    if mask is None:
+        return result
+    import scipy.ndimage as sndi
+
+    mask = np.asarray(mask)
+    eroded = sndi.binary_erosion(mask, np.ones((3,) * mask.ndim, bool), border_value=0)
+    return (result * eroded).astype(result.dtype)
+
+
 def sk_sobel(image, mask=None, *, axis=None, mode="reflect", cval=0.0):
-    return generic_edge_filter(image, smooth_weights=_SOBEL_SMOOTH, axis=axis, mode=mode)
+    return mask_filter_result(
+        generic_edge_filter(image, smooth_weights=_SOBEL_SMOOTH, axis=axis, mode=mode), mask)
 
 
 def sk_prewitt(image, mask=None, *, axis=None, mode="reflect", cval=0.0):
-    return generic_edge_filter(image, smooth_weights=_PREWITT_SMOOTH, axis=axis, mode=mode)
+    return mask_filter_result(
+        generic_edge_filter(image, smooth_weights=_PREWITT_SMOOTH, axis=axis, mode=mode), mask)
+
+
+def sk_scharr(image, mask=None, *, axis=None, mode="reflect", cval=0.0):
+    """filters/edges.py:362-422."""
+    return mask_filter_result(
+        generic_edge_filter(image, smooth_weights=_SCHARR_SMOOTH, axis=axis, mode=mode), mask)
+
+
+def sk_farid(image, mask=None, *, axis=None, mode="reflect", cval=0.0):
+    """filters/edges.py:783-850."""
+    return mask_filter_result(
+        generic_edge_filter(image, smooth_weights=_FARID_SMOOTH, edge_weights=_FARID_EDGE,
+                            axis=axis, mode=mode), mask)
 
 
 def hessian_matrix_gaussian(image, sigma=1, mode="reflect", cval=0, order="rc"):
