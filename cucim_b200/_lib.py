@@ -173,6 +173,10 @@ _sigs = {
     ),
     "cimx_nonpositive_to_one": ([_A, ctypes.c_void_p], ctypes.c_int),
     "cimx_mask_erode_multiply": ([_A, _A, ctypes.c_void_p], ctypes.c_int),
+    "cimx_multiply": ([_A, _A, _A, ctypes.c_void_p], ctypes.c_int),
+    "cimx_corner_response": (
+        [ctypes.c_int, _A, ctypes.c_int, _A, _A, ctypes.c_double, ctypes.c_void_p], ctypes.c_int,
+    ),
     "cimx_ridge_filter": (
         [_A, _A, ctypes.c_int, _P(ctypes.c_double), ctypes.c_int, ctypes.c_double,
          ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_double,
@@ -194,6 +198,9 @@ EXPORTED = tuple(_sigs)
 
 COMBINE_ADD = 0
 COMBINE_SUBTRACT = 1
+
+CORNER_KITCHEN_ROSENFELD, CORNER_HARRIS_K, CORNER_HARRIS_EPS, CORNER_SHI_TOMASI, \
+    CORNER_FOERSTNER = range(5)
 
 
 def last_error():

@@ -1,5 +1,6 @@
-"""hessian_matrix and its eigenvalues from cucim.skimage.feature
-(python/cucim/src/cucim/skimage/feature/corner.py:161-362, :473-837)."""
+"""hessian_matrix, structure_tensor, their eigenvalues and the corner
+measures of cucim.skimage.feature (python/cucim/src/cucim/skimage/feature/
+corner.py:21-158, :161-384, :473-858, :940-1284)."""
 
 import ctypes
 import math
@@ -13,7 +14,9 @@ from .. import ndimage as ndi
 from .._util import supported_float_type
 from . import util as _u
 
-__all__ = ["hessian_matrix", "hessian_matrix_eigvals"]
+__all__ = ["hessian_matrix", "hessian_matrix_eigvals", "structure_tensor",
+           "structure_tensor_eigenvalues", "corner_kitchen_rosenfeld", "corner_harris",
+           "corner_shi_tomasi", "corner_foerstner"]
 
 
 def _as_float_image(image):
@@ -122,3 +125,105 @@ def symmetric_compute_eigenvalues(S_elems, sort="descending", abs_sort=False):
 def hessian_matrix_eigvals(H_elems):
     """corner.py:824-858: eigenvalues in decreasing order, leading axis."""
     return symmetric_compute_eigenvalues(H_elems)
+
+
+# ------------------------------------------------ structure tensor, corners
+
+def _prepare_grayscale_input_nd(image):
+    """feature/util.py:19-24: squeeze, 2-5 dimensions, img_as_float, the
+    supported float type."""
+    x = _arrays.as_tensor(image)
+    x = x.squeeze()
+    if x.dim() not in range(2, 6):
+        raise ValueError("The parameter `image` must be a 2-, 3-, 4- or 5-dimensional array")
+    return _as_float_image(x)
+
+
+def _compute_derivatives(image, mode="constant", cval=0):
+    """corner.py:21-45: the ndimage sobel along every axis."""
+    ndim = _arrays.as_tensor(image).dim()
+    return [ndi.sobel(image, axis=i, mode=mode, cval=cval) for i in range(ndim)]
+
+
+def _multiply(a, b):
+    ta, tb = _arrays.as_tensor(a).contiguous(), _arrays.as_tensor(b).contiguous()
+    out = _arrays.empty(ta.shape, _arrays.np_dtype(ta), ta.device)
+    ca, cb, co = _arrays.to_cimx(ta), _arrays.to_cimx(tb), _arrays.to_cimx(out)
+    _lib.check(_lib.lib.cimx_multiply(ctypes.byref(ca), ctypes.byref(cb), ctypes.byref(co),
+                                      _arrays.stream_of(ta)), "multiply")
+    return out
+
+
+def structure_tensor(image, sigma=1, mode="constant", cval=0, order="rc"):
+    """corner.py:48-158: the Gaussian-weighted products of the sobel
+    derivatives, upper-triangular elements in combinations_with_replacement
+    order (Arr, Arc, Acc for 2-D)."""
+    from .filters import gaussian  # noqa: PLC0415
+
+    x = _arrays.as_tensor(image)
+    if order == "xy" and x.dim() > 2:
+        raise ValueError('Only "rc" order is supported for dim > 2.')
+    if order not in ["rc", "xy"]:
+        raise ValueError(f'order {order} is invalid. Must be either "rc" or "xy"')
+    if not np.isscalar(sigma):
+        sigma = tuple(sigma)
+        if len(sigma) != x.dim():
+            raise ValueError("sigma must have as many elements as image has axes")
+    image = _prepare_grayscale_input_nd(image)
+    derivatives = _compute_derivatives(image, mode=mode, cval=cval)
+    if order == "xy":
+        derivatives = list(reversed(derivatives))
+    t = _arrays.as_tensor(image)
+    channel_axis = -1 if (t.dim() == 3 and t.shape[-1] == 3) else None
+    return [gaussian(_multiply(d0, d1), sigma=sigma, mode=mode, cval=cval,
+                     channel_axis=channel_axis)
+            for d0, d1 in combinations_with_replacement(derivatives, 2)]
+
+
+def structure_tensor_eigenvalues(A_elems):
+    """corner.py:786-821: eigenvalues in decreasing order, leading axis."""
+    return symmetric_compute_eigenvalues(A_elems)
+
+
+def _corner(kind, inputs, n_out=1, param=0.0):
+    ts = [_arrays.as_tensor(i).contiguous() for i in inputs]
+    outs = [_arrays.empty(ts[0].shape, _arrays.np_dtype(ts[0]), ts[0].device)
+            for _ in range(n_out)]
+    arr = (_lib.CimxArray * len(ts))(*[_arrays.to_cimx(t) for t in ts])
+    co = [_arrays.to_cimx(o) for o in outs]
+    rc = _lib.lib.cimx_corner_response(kind, arr, len(ts), ctypes.byref(co[0]),
+                                       ctypes.byref(co[1]) if n_out > 1 else None,
+                                       float(param), _arrays.stream_of(ts[0]))
+    _lib.check(rc, "corner response")
+    return [_arrays.wrap_like(inputs[0], o) for o in outs]
+
+
+def corner_kitchen_rosenfeld(image, mode="constant", cval=0):
+    """corner.py:962-1004."""
+    fdt = supported_float_type(_arrays.np_dtype(_arrays.as_tensor(image)))
+    image = _u.astype(image, fdt)
+    imy, imx = _compute_derivatives(image, mode=mode, cval=cval)
+    imxy, imxx = _compute_derivatives(imx, mode=mode, cval=cval)
+    imyy = ndi.sobel(imy, axis=0, mode=mode, cval=cval)
+    return _corner(_lib.CORNER_KITCHEN_ROSENFELD, [imx, imy, imxx, imxy, imyy])[0]
+
+
+def corner_harris(image, method="k", k=0.05, eps=1e-6, sigma=1):
+    """corner.py:1041-1113."""
+    Arr, Arc, Acc = structure_tensor(image, sigma, order="rc")
+    if method == "k":
+        return _corner(_lib.CORNER_HARRIS_K, [Arr, Acc, Arc], param=k)[0]
+    return _corner(_lib.CORNER_HARRIS_EPS, [Arr, Acc, Arc], param=eps)[0]
+
+
+def corner_shi_tomasi(image, sigma=1):
+    """corner.py:1131-1189."""
+    Arr, Arc, Acc = structure_tensor(image, sigma, order="rc")
+    return _corner(_lib.CORNER_SHI_TOMASI, [Arr, Acc, Arc])[0]
+
+
+def corner_foerstner(image, sigma=1):
+    """corner.py:1216-1284: (w, q)."""
+    Arr, Arc, Acc = structure_tensor(image, sigma, order="rc")
+    w, q = _corner(_lib.CORNER_FOERSTNER, [Arr, Acc, Arc], n_out=2)
+    return w, q

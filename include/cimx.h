@@ -405,6 +405,30 @@ CIMX_API int cimx_nonpositive_to_one(const CimxArray* a, void* stream);
 CIMX_API int cimx_mask_erode_multiply(const CimxArray* result, const CimxArray* mask,
                                       void* stream);
 
+/* out = a * b elementwise (float32/float64, equal shapes, C-contiguous): the
+ * derivative products of structure_tensor (feature/corner.py:146-156). */
+CIMX_API int cimx_multiply(const CimxArray* a, const CimxArray* b, const CimxArray* out,
+                           void* stream);
+
+/* Corner measures of feature/corner.py from their input images (all of one
+ * float dtype and shape, C-contiguous):
+ *   CIMX_CORNER_KITCHEN_ROSENFELD  inputs imx, imy, imxx, imxy, imyy (:940-1004);
+ *   CIMX_CORNER_HARRIS_K           inputs Arr, Acc, Arc; param = k   (:1007-1021);
+ *   CIMX_CORNER_HARRIS_EPS         inputs Arr, Acc, Arc; param = eps (:1024-1038);
+ *   CIMX_CORNER_SHI_TOMASI         inputs Arr, Acc, Arc              (:1116-1128);
+ *   CIMX_CORNER_FOERSTNER          inputs Arr, Acc, Arc; out = w, out2 = q (:1192-1213).
+ * Each evaluates cuCIM's kernel expression in the same types. */
+enum {
+  CIMX_CORNER_KITCHEN_ROSENFELD = 0,
+  CIMX_CORNER_HARRIS_K = 1,
+  CIMX_CORNER_HARRIS_EPS = 2,
+  CIMX_CORNER_SHI_TOMASI = 3,
+  CIMX_CORNER_FOERSTNER = 4,
+};
+CIMX_API int cimx_corner_response(int kind, const CimxArray* inputs, int ninputs,
+                                  const CimxArray* out, const CimxArray* out2, double param,
+                                  void* stream);
+
 /* One tile of a batch for cimx_batch_gray_gauss_sobel. */
 typedef struct CimxBatchTile {
   const uint8_t* rgb;   /* device: height x width x 3 uint8, C-contiguous */

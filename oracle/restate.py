@@ -809,10 +809,12 @@ def eigvals_sym(elems, sort="descending", abs_sort=False):
     e = [np.asarray(x, dtype=np.float64) for x in elems]
     if len(e) == 3:
         m00, m01, m11 = e
-        # the 2x2 kernel keeps its temporaries in F
+        # the 2x2 kernel keeps its temporaries in F; the CUDA compiler fuses
+        # `tmp2 *= tmp2; tmp2 += tmp1;` into one fused multiply-add in F
+        # (nvcc's and NVRTC's default --fmad=true contracts across statements)
         t1 = (m01 * m01).astype(F) * F.type(4)
         t2 = (m00 - m11).astype(F)
-        t2 = (t2 * t2 + t1).astype(F)
+        t2 = fma(t2, t2, t1.astype(F))
         t2 = (np.sqrt(t2) / F.type(2)).astype(F)
         t1 = ((m00 + m11).astype(F) / F.type(2)).astype(F)
         lo, hi = (t1 - t2).astype(F), (t1 + t2).astype(F)
@@ -877,9 +879,11 @@ def _by_chunks(fn, arrays):
 
 
 def _frangi_rg(ev, F):
-    rg = np.zeros(ev.shape[1:], F)
-    for lam in ev:
-        rg = (rg + lam.astype(np.float64) * lam).astype(F)
+    """r_g = l0*l0, then r_g += l*l for the others (ridges.py:228-263), each
+    += fused with its product by the compiler."""
+    rg = (ev[0] * ev[0]).astype(F)
+    for lam in ev[1:]:
+        rg = fma(lam, lam, rg)
     return rg
 
 
@@ -1006,6 +1010,69 @@ def hessian_ridge(image, sigmas=range(1, 10, 2), alpha=0.5, beta=0.5, gamma=15,
                  black_ridges=black_ridges, mode=mode, cval=cval)
     out[out <= 0] = 1
     return out
+
+
+def structure_tensor(image, sigma=1, mode="constant", cval=0, order="rc"):
+    """feature/corner.py:48-158 (with feature/util.py:19-24 for the input)."""
+    image = np.squeeze(np.asarray(image))
+    image = img_as_float(image)
+    image = image.astype(supported_float_type(image.dtype), copy=False)
+    F = image.dtype
+    ders = [sobel(image, i, mode=mode, cval=cval) for i in range(image.ndim)]
+    if order == "xy":
+        ders = ders[::-1]
+    channel_axis = -1 if (image.ndim == 3 and image.shape[-1] == 3) else None
+    return [sk_gaussian((d0 * d1).astype(F), sigma=sigma, mode=mode, cval=cval,
+                        channel_axis=channel_axis)
+            for d0, d1 in combinations_with_replacement(ders, 2)]
+
+
+def corner_kitchen_rosenfeld(image, mode="constant", cval=0):
+    """feature/corner.py:940-1004 (no contraction: compared with a tolerance)."""
+    image = np.asarray(image)
+    image = image.astype(supported_float_type(image.dtype), copy=False)
+    imy, imx = (sobel(image, i, mode=mode, cval=cval) for i in range(2))
+    imxy, imxx = (sobel(imx, i, mode=mode, cval=cval) for i in range(2))
+    imyy = sobel(imy, 0, mode=mode, cval=cval)
+    F = image.dtype
+    den = (imx * imx + imy * imy).astype(F)
+    num = imxx * (imy * imy) + imyy * (imx * imx) - 2 * imxy * imx * imy
+    with np.errstate(divide="ignore", invalid="ignore"):
+        r = np.where(den == 0, 0, num / np.where(den == 0, 1, den))
+    return r.astype(F)
+
+
+def corner_harris(image, method="k", k=0.05, eps=1e-6, sigma=1):
+    """feature/corner.py:1007-1113."""
+    Arr, Arc, Acc = structure_tensor(image, sigma)
+    F = Arr.dtype
+    det = (Arr * Acc - Arc * Arc).astype(F)
+    tr = (Arr + Acc).astype(F)
+    if method == "k":
+        r = det.astype(np.float64) - k * tr.astype(np.float64) * tr
+    else:
+        r = 2 * det.astype(np.float64) / (tr.astype(np.float64) + eps)
+    return r.astype(F)
+
+
+def corner_shi_tomasi(image, sigma=1):
+    """feature/corner.py:1116-1189."""
+    Arr, Arc, Acc = structure_tensor(image, sigma)
+    F = Arr.dtype
+    tmp = ((Arr - Acc) * (Arr - Acc)).astype(F)
+    return ((Arr + Acc - np.sqrt(tmp + 4 * Arc * Arc)) / 2.0).astype(F)
+
+
+def corner_foerstner(image, sigma=1):
+    """feature/corner.py:1192-1284."""
+    Arr, Arc, Acc = structure_tensor(image, sigma)
+    F = Arr.dtype
+    det = (Arr * Acc - Arc * Arc).astype(F)
+    tr = (Arr + Acc).astype(F)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        w = np.where(tr == 0, 0, det / tr).astype(F)
+        q = np.where(tr == 0, 0, 4 * det / (tr * tr)).astype(F)
+    return w, q
 
 
 def rgb2gray(rgb, channel_axis=-1):
