@@ -318,13 +318,27 @@ __global__ void k_gradient(const F* __restrict__ f, F* __restrict__ g, int64_t o
 }
 
 // frangi epilogue for one scale (filters/ridges.py:228-319, :436-475):
-// r_g = sum of squared eigenvalues (kept in F, contracted like cuCIM's
-// `r_g += l*l`), gamma from the first scale's max(r_g), the vesselness
-// formula with float64 exponentials, and the running maximum over scales.
+// r_g = sum of squared eigenvalues in F, gamma from the first scale's
+// max(r_g), the vesselness formula with float64 exponentials, and the
+// running maximum over scales.
+//
+// cuCIM's sum kernels are `r_g = l1 * l1; r_g += l2 * l2; [r_g += l3 * l3;]`
+// compiled with contraction on: the CUDA compiler fuses the first product
+// into the first addition, fma(l1, l1, l2 * l2) (on 1 M GPU results of the
+// compiled 2-D statements, that form matched all and the other two
+// associations did not), and the third product into the second addition. Written out with explicit
+// fused multiply-adds so that no loop or inlining decision can change it.
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+
 template <class F>
 __device__ __forceinline__ F frangi_rg(const F* const* ev, int nd, int64_t i) {
-  F r = ev[0][i] * ev[0][i];
-  for (int k = 1; k < nd; ++k) r += ev[k][i] * ev[k][i];
+  const F l1 = ev[0][i], l2 = ev[1][i];
+  F r = fma(l1, l1, mul_rn(l2, l2));
+  if (nd == 3) {
+    const F l3 = ev[2][i];
+    r = fma(l3, l3, r);
+  }
   return r;
 }
 

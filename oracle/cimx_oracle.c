@@ -471,3 +471,48 @@ void oracle_fma(const void* a, const void* b, const void* c, int64_t n, int w64,
       ((float*)out)[i] = fmaf(((const float*)a)[i], ((const float*)b)[i], ((const float*)c)[i]);
   }
 }
+
+/* One scale of frangi's epilogue (filters/ridges.py:228-319): the sum of
+ * squared eigenvalues r_g and the vesselness, for n voxels of nd = 2 or 3
+ * eigenvalue images sorted ascending by magnitude, float32 (w64 == 0) or
+ * float64. cuCIM's kernels compute r_g = l1*l1; r_g += l2*l2; (r_g += l3*l3;)
+ * with the CUDA compiler's contraction, fma(l1, l1, l2*l2) then
+ * fma(l3, l3, .), and the exponentials in double with the C math library's
+ * exp, which agreed with the GPU's on every one of 2 M voxels. rg (if not
+ * NULL) receives r_g; v the vesselness of this scale. */
+#define ORACLE_FRANGI_BODY(F, FMA, FMAX, FABS)                                      \
+  for (int64_t i = 0; i < n; ++i) {                                                 \
+    const F e1 = ((const F*)l1)[i], e2 = ((const F*)l2)[i];                         \
+    const F e3 = nd == 3 ? ((const F*)l3)[i] : (F)0;                                \
+    F r_g = FMA(e1, e1, e2 * e2);                                                   \
+    if (nd == 3) r_g = FMA(e3, e3, r_g);                                            \
+    if (rg) ((F*)rg)[i] = r_g;                                                      \
+    if (!v) continue;                                                               \
+    F result;                                                                       \
+    if (nd == 2) {                                                                  \
+      F r_b = FABS(e1) / FMAX(e2, (F)1.0e-10);                                      \
+      r_b = r_b * r_b;                                                              \
+      result = (F)exp(-(double)r_b / beta_sq);                                      \
+      result = (F)((double)result * (1.0 - exp(-(double)r_g / gamma_sq)));         \
+    } else {                                                                        \
+      const F lam2 = FMAX(e2, (F)1.0e-10), lam3 = FMAX(e3, (F)1.0e-10);             \
+      F r_a = lam2 / lam3;                                                          \
+      r_a = r_a * r_a;                                                              \
+      const F r_b = (e1 * e1) / (lam2 * lam3);                                      \
+      result = (F)(1.0 - exp(-(double)r_a / alpha_sq));                             \
+      result = (F)((double)result * exp(-(double)r_b / beta_sq));                   \
+      result = (F)((double)result * (1.0 - exp(-(double)r_g / gamma_sq)));         \
+    }                                                                               \
+    ((F*)v)[i] = result;                                                            \
+  }
+
+void oracle_frangi_scale(const void* l1, const void* l2, const void* l3, int nd, int64_t n,
+                         int w64, double alpha_sq, double beta_sq, double gamma_sq, void* rg,
+                         void* v) {
+  if (w64) {
+    ORACLE_FRANGI_BODY(double, fma, fmax, fabs)
+  } else {
+    ORACLE_FRANGI_BODY(float, fmaf, fmaxf, fabsf)
+  }
+}
+#undef ORACLE_FRANGI_BODY
