@@ -6,6 +6,6 @@ call the sm_100a kernels of libcimx.so through its C ABI (include/cimx.h).
 """
 
 from . import _lib  # noqa: F401  (raises if libcimx.so is missing)
-from . import ndimage, skimage  # noqa: F401
+from . import ndimage, skimage, tune  # noqa: F401
 
 __version__ = "0.1.0"

@@ -40,6 +40,11 @@ L_NO_FUSION = 1 << 0
 L_TENSOR_BF16X3 = 1 << 1
 L_TENSOR_TF32X3 = 1 << 2
 L_TENSOR_ALL_LINES = 1 << 3
+L_NO_VOLUME = 1 << 4
+L_NO_STREAM = 1 << 5
+L_NO_ROWSTREAM = 1 << 6
+L_NO_TUNE = 1 << 7
+L_ZCHUNK_SHIFT = 8
 
 E_INVALID, E_DTYPE, E_CUDA, E_NOMEM, E_LAYOUT, E_TIMEOUT = -1, -2, -3, -4, -5, -6
 
@@ -87,6 +92,11 @@ _sigs = {
     "cimx_set_allocator": ([ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
     "cimx_device_status": ([ctypes.c_int], ctypes.c_int),
     "cimx_wait_selftest": ([ctypes.c_int, ctypes.c_longlong, ctypes.c_void_p], ctypes.c_int),
+    "cimx_tune_mode": ([ctypes.c_int], ctypes.c_int),
+    "cimx_tune_load": ([ctypes.c_char_p], ctypes.c_int),
+    "cimx_tune_save": ([ctypes.c_char_p], ctypes.c_int),
+    "cimx_tune_clear": ([], ctypes.c_int),
+    "cimx_tune_dump": ([ctypes.c_char_p, ctypes.c_longlong], ctypes.c_longlong),
     "cimx_correlate1d": (
         [_A, _A, _P(ctypes.c_double), ctypes.c_int, ctypes.c_int, ctypes.c_int,
          ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_void_p],

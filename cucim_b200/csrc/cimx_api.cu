@@ -245,6 +245,14 @@ int cimx_separable(const CimxArray* in, const CimxArray* out, const CimxPass* pa
   }
   if (n == 0) return CIMX_OK;
 
+  // the autotuner's schedule for this signature (or the caller's flags)
+  if (!(lib_flags & CIMX_L_NO_TUNE)) {
+    const std::string key = tune_key(in, out, ds.data(), npasses, lib_flags);
+    lib_flags = tuned_flags(key, lib_flags, st, [&](int f) {
+      return cimx_separable(in, out, passes, npasses, f, stream);
+    });
+  }
+
   const bool tf32x3 = (lib_flags & CIMX_L_TENSOR_TF32X3) != 0;
   const bool tensor = tf32x3 || (lib_flags & CIMX_L_TENSOR_BF16X3) != 0;
   // Tensor-core passes where they measured faster than the plain kernels: on
@@ -269,7 +277,7 @@ int cimx_separable(const CimxArray* in, const CimxArray* out, const CimxPass* pa
   }
   // fused kernels take whole runs of passes in one launch
   if (!any_tensor && !(lib_flags & CIMX_L_NO_FUSION)) {
-    rc = try_fused(in, out, ds.data(), npasses, st);
+    rc = try_fused(in, out, ds.data(), npasses, lib_flags, st);
     if (rc != CIMX_FUSED_DECLINED) return rc;
     rc = CIMX_OK;
   }

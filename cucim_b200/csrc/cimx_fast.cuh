@@ -964,7 +964,7 @@ int launch_rowstream_k(const SlabArgs& s, cudaStream_t st) {
 
 template <class T, class D>
 bool rowstream_fits(const SlabArgs& s) {
-  if (!s.has_x || !s.has_y || s.py.K != s.px.K) return false;
+  if (s.no_rowstream || !s.has_x || !s.has_y || s.py.K != s.px.K) return false;
   if (s.X % 4 != 0 || s.X < 4 || s.Y < 1) return false;
   // measured on a 512 x 1024 x 1024 float32 stack: 4.0 / 3.1 TB/s for 3 / 5
   // taps, faster than the slab kernel; 9 and 17 taps run at 1.7 / 0.94 TB/s,

@@ -104,7 +104,8 @@ int launch_vol(const VolArgs& v, int tin, int tout, cudaStream_t st) {
 
 // z, y and x passes over the last three axes with the same short taps: one
 // launch of the volume kernel, no intermediate volume
-int try_vol(const CimxArray* in, const CimxArray* out, const PassDesc* ds, cudaStream_t st) {
+int try_vol(const CimxArray* in, const CimxArray* out, const PassDesc* ds, int zchunk,
+            cudaStream_t st) {
   const int nd = in->ndim;
   const int D = out->dtype;
   if (!fast_pair(in->dtype, D)) return CIMX_FUSED_DECLINED;
@@ -130,6 +131,7 @@ int try_vol(const CimxArray* in, const CimxArray* out, const PassDesc* ds, cudaS
   v.Z = Z;
   v.Y = Y;
   v.X = X;
+  v.zchunk = zchunk;
   fill_slab_pass(v.pz, ds[0], t[0], in->dtype);
   fill_slab_pass(v.py, ds[1], t[1], D);
   fill_slab_pass(v.px, ds[2], t[2], D);
@@ -139,7 +141,7 @@ int try_vol(const CimxArray* in, const CimxArray* out, const PassDesc* ds, cudaS
 }  // namespace
 
 int try_fused(const CimxArray* in, const CimxArray* out, PassDesc* ds, int npasses,
-              cudaStream_t st) {
+              int lib_flags, cudaStream_t st) {
   const int nd = in->ndim;
   const int D = out->dtype;
   if (npasses < 1 || nd < 1) return CIMX_FUSED_DECLINED;
@@ -151,8 +153,9 @@ int try_fused(const CimxArray* in, const CimxArray* out, PassDesc* ds, int npass
   }
 
   if (nd >= 3 && npasses == 3 && ds[0].axis == nd - 3 && ds[1].axis == nd - 2 &&
-      ds[2].axis == nd - 1) {
-    const int rc = try_vol(in, out, ds, st);
+      ds[2].axis == nd - 1 && !(lib_flags & CIMX_L_NO_VOLUME)) {
+    static const int kChunks[4] = {0, 32, 64, 128};
+    const int rc = try_vol(in, out, ds, kChunks[(lib_flags >> CIMX_L_ZCHUNK_SHIFT) & 3], st);
     if (rc != CIMX_FUSED_DECLINED) return rc;
   }
 
@@ -169,8 +172,9 @@ int try_fused(const CimxArray* in, const CimxArray* out, PassDesc* ds, int npass
   for (size_t n = 0; n < lead.size(); ++n) {
     const int i = lead[n];
     const int tin = n == 0 ? in->dtype : D;
-    const bool stream_ok = trim(ds[i], 17, tr[i]) && stream_supports(tr[i].K) &&
-                           fast_pair(tin, D) && ds[i].inner % 4 == 0;
+    const bool stream_ok = !(lib_flags & CIMX_L_NO_STREAM) && trim(ds[i], 17, tr[i]) &&
+                           stream_supports(tr[i].K) && fast_pair(tin, D) &&
+                           ds[i].inner % 4 == 0;
     if (!stream_ok) {
       if (tail.empty()) return CIMX_FUSED_DECLINED;
       lead_generic[i] = 1;
@@ -221,6 +225,7 @@ int try_fused(const CimxArray* in, const CimxArray* out, PassDesc* ds, int npass
   }
   if (rc == CIMX_OK && !tail.empty()) {
     SlabArgs a{};
+    a.no_rowstream = (lib_flags & CIMX_L_NO_ROWSTREAM) ? 1 : 0;
     a.in = src;
     a.out = dst_of(j++);
     a.X = in->shape[nd - 1];

@@ -29,6 +29,7 @@ struct SlabArgs {
   long long tiles_x, tiles_y;
   int has_y, has_x;
   int* status;  // device status word for bounded waits
+  int no_rowstream;  // CIMX_L_NO_ROWSTREAM: always the slab kernel
   SlabPass py, px;
 };
 
@@ -38,6 +39,7 @@ struct VolArgs {
   const void* in;
   void* out;
   long long B, Z, Y, X;
+  int zchunk;  // slices per CTA; 0: chosen from the grid size
   SlabPass pz, py, px;
 };
 
@@ -45,7 +47,7 @@ struct VolArgs {
 // in fast launches when they cover it. Returns CIMX_OK, a negative error, or
 // CIMX_FUSED_DECLINED (nothing was launched).
 int try_fused(const CimxArray* in, const CimxArray* out, PassDesc* ds, int npasses,
-              cudaStream_t stream);
+              int lib_flags, cudaStream_t stream);
 
 // elementwise copy with conversion (used when a filter has no passes)
 int launch_copy_cast(const void* in, int tin, void* out, int tout, int64_t n,

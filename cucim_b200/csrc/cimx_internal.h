@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -52,6 +53,15 @@ int make_pass(const CimxArray* shape_of, const CimxPass& p, std::vector<double>&
 // scratch memory through the installed allocator
 void* scratch_alloc(size_t nbytes, cudaStream_t s);
 void scratch_free(void* p, size_t nbytes, cudaStream_t s);
+
+// The autotuner (cimx_tune.cu): the table key of a resolved pass list, and
+// the library flags to run it with (the caller's, or the tuned schedule;
+// with tuning on and an unseen key, `run(flags)` is timed for every
+// candidate schedule first).
+std::string tune_key(const CimxArray* in, const CimxArray* out, const PassDesc* ds,
+                     int npasses, int lib_flags);
+int tuned_flags(const std::string& key, int lib_flags, cudaStream_t st,
+                const std::function<int(int)>& run);
 
 // generic single pass (cimx_pass.cu)
 int launch_generic_pass(const PassDesc& d, cudaStream_t stream);

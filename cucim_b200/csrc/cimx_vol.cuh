@@ -377,6 +377,7 @@ int launch_vol_km(const VolArgs& v, cudaStream_t st) {
   const long long waves = K == 3 ? 12 : 6;
   int zc = 128;
   while (zc > 16 && tiles * ((v.Z + zc - 1) / zc) * v.B < 148LL * waves) zc /= 2;
+  if (v.zchunk > 0) zc = v.zchunk;  // a tuned or forced chunk (any chunk is exact)
   a.zchunk = zc;
   const long long nzc = (v.Z + zc - 1) / zc;
   if (tiles > 0x7fffffffLL || nzc > 65535) return CIMX_FUSED_DECLINED;

@@ -118,6 +118,21 @@ def pass_by_pass():
         _EXTRA_LIB_FLAGS = old
 
 
+@contextlib.contextmanager
+def schedule(lib_flags):
+    """Within this block every filter runs with the given CIMX_L_* schedule
+    flags (for example _lib.L_NO_VOLUME | _lib.L_NO_ROWSTREAM), which the
+    autotuner then leaves alone. All schedules give bit-identical results;
+    a testing and measurement aid, not thread-safe."""
+    global _EXTRA_LIB_FLAGS
+    old = _EXTRA_LIB_FLAGS
+    _EXTRA_LIB_FLAGS = old | int(lib_flags)
+    try:
+        yield
+    finally:
+        _EXTRA_LIB_FLAGS = old
+
+
 def _hashable(obj):
     """`obj` with lists turned into tuples, or None when it cannot be a key."""
     if isinstance(obj, (list, tuple)):

@@ -82,6 +82,15 @@ enum {
                                    faster; takes precedence when both bits are set */
   CIMX_L_TENSOR_ALL_LINES = 1 << 3,/* with a tensor bit: every eligible pass on the tensor
                                    cores whatever its line length (testing, measurement) */
+  /* Schedule choices. Each selects between kernels that give bit-identical
+   * results; the autotuner (cimx_tune_*) picks among them per call signature. */
+  CIMX_L_NO_VOLUME = 1 << 4,    /* 3-D short filters: stream + slab launches instead of the
+                                   single-launch volume kernel */
+  CIMX_L_NO_STREAM = 1 << 5,    /* leading-axis passes on the generic kernel, not k_stream */
+  CIMX_L_NO_ROWSTREAM = 1 << 6, /* (y, x) passes on the slab kernel, not the row stream */
+  CIMX_L_NO_TUNE = 1 << 7,      /* this call neither consults nor fills the tuning table */
+  CIMX_L_ZCHUNK_SHIFT = 8,      /* bits 8-9: volume-kernel z chunk, 0 = automatic,
+                                   1/2/3 = 32/64/128 slices */
 };
 
 /* One 1-D correlation pass of a separable filter. */
@@ -133,6 +142,35 @@ CIMX_API int cimx_wait_selftest(int which, long long limit, void* stream);
 typedef void* (*cimx_alloc_fn)(size_t nbytes, void* stream, void* user);
 typedef void (*cimx_free_fn)(void* ptr, size_t nbytes, void* stream, void* user);
 CIMX_API int cimx_set_allocator(cimx_alloc_fn alloc, cimx_free_fn release, void* user);
+
+/* The schedule autotuner of cimx_separable (and of every entry built on
+ * it). A pass list can run on several kernel schedules with bit-identical
+ * results (CIMX_L_NO_VOLUME, CIMX_L_NO_STREAM, CIMX_L_NO_ROWSTREAM,
+ * CIMX_L_NO_FUSION, the z chunk bits); with a tensor flag the tensor-core
+ * and plain passes are candidates too. The tuner keys a table on the call
+ * signature (dtypes, shape, each pass's axis, taps, anchor, mode and flags,
+ * the tensor flags), one table per device model:
+ *   CIMX_TUNE_OFF  the built-in rules only;
+ *   CIMX_TUNE_USE  recorded schedules where present (the default);
+ *   CIMX_TUNE_ON   an unseen signature is timed on the call's own arrays (each
+ *                  candidate once to warm up and three times between CUDA
+ *                  events; this synchronises the stream, and is skipped while
+ *                  the stream is being captured) and the fastest recorded.
+ * A call that sets a schedule flag itself, or CIMX_L_NO_TUNE, is not tuned.
+ * Environment: CIMX_TUNE = 0/1/2 sets the initial mode; CIMX_TUNE_CACHE
+ * names a JSON file read at first use and rewritten after each newly tuned
+ * signature. cuCIM chooses its kernel by a fixed rule instead
+ * (_vendored/_ndimage_filters.py:284-297); no counterpart there. */
+enum { CIMX_TUNE_OFF = 0, CIMX_TUNE_USE = 1, CIMX_TUNE_ON = 2 };
+/* Sets the mode (mode < 0: leaves it) and returns the previous one. */
+CIMX_API int cimx_tune_mode(int mode);
+/* Merges the entries of a JSON table file; writes the whole table. */
+CIMX_API int cimx_tune_load(const char* path);
+CIMX_API int cimx_tune_save(const char* path);
+CIMX_API int cimx_tune_clear(void);
+/* The table as JSON text into buf (truncated to size - 1 characters, NUL
+ * terminated); returns the size the whole text needs, NUL included. */
+CIMX_API long long cimx_tune_dump(char* buf, long long size);
 
 /* One 1-D correlation (or convolution) along `axis`.
  * Replaces the shared-memory kernel driver _shmem_convolve1d
