@@ -193,6 +193,11 @@ _sigs = {
          ctypes.c_int, ctypes.c_void_p],
         ctypes.c_int,
     ),
+    "cimx_frangi_hessian_accumulate": (
+        [_A, ctypes.c_int, _A, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+         ctypes.c_void_p, ctypes.c_void_p],
+        ctypes.c_int,
+    ),
     "cimx_frangi_accumulate": (
         [_A, ctypes.c_int, _A, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int,
          ctypes.c_void_p, ctypes.c_void_p],

@@ -330,6 +330,8 @@ __global__ void k_gradient(const F* __restrict__ f, F* __restrict__ g, int64_t o
 // fused multiply-adds so that no loop or inlining decision can change it.
 __device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
 __device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
 
 template <class F>
 __device__ __forceinline__ F frangi_rg(const F* const* ev, int nd, int64_t i) {
@@ -363,48 +365,109 @@ __global__ void k_frangi_max_rg(const F* __restrict__ l0, const F* __restrict__ 
   }
 }
 
+// gamma^2 of the automatic gamma: half the square root of the first scale's
+// largest r_g (ridges.py:447-453), or the fixed value
+__device__ __forceinline__ double frangi_gamma_sq(double gamma_sq_fixed,
+                                                  const unsigned long long* maxbits) {
+  if (!maxbits) return gamma_sq_fixed;
+  const double s_max = __longlong_as_double(static_cast<long long>(*maxbits));
+  const double gamma = sqrt(s_max) / 2.0;
+  return (s_max == 0) ? 2.0 : max(2 * gamma * gamma, 1e-10);
+}
+
+// The vesselness of one voxel from its eigenvalues (ascending by magnitude)
+// and r_g: cuCIM's 2-D and 3-D inner kernels, statement by statement.
+template <class F>
+__device__ __forceinline__ F frangi_value(F lambda1, F lambda2, F lambda3, int nd, F r_g,
+                                          double alpha_sq, double beta_sq, double gamma_sq) {
+  F result;
+  if (nd == 2) {
+    F r_b;
+    r_b = abs(lambda1) / max(lambda2, static_cast<F>(1.0e-10));
+    r_b *= r_b;
+    result = exp(-r_b / beta_sq);
+    result *= 1.0 - exp(-r_g / gamma_sq);
+  } else {
+    F r_a, r_b;
+    F lam2 = max(lambda2, static_cast<F>(1.0e-10));
+    F lam3 = max(lambda3, static_cast<F>(1.0e-10));
+    r_a = lam2 / lam3;
+    r_a *= r_a;
+    r_b = (lambda1 * lambda1) / (lam2 * lam3);
+    result = 1.0 - exp(-r_a / alpha_sq);
+    result *= exp(-r_b / beta_sq);
+    result *= 1.0 - exp(-r_g / gamma_sq);
+  }
+  return result;
+}
+
+// cupy.maximum: NaN in either operand propagates
+template <class F>
+__device__ __forceinline__ F frangi_fold(F prev, F result) {
+  return (prev != prev) ? prev : ((result != result) ? result : (prev > result ? prev : result));
+}
+
 template <class F>
 __global__ void k_frangi_inner(const F* __restrict__ l0, const F* __restrict__ l1,
                                const F* __restrict__ l2, int nd, int64_t n, double alpha_sq,
                                double beta_sq, double gamma_sq_fixed,
                                const unsigned long long* maxbits, F* out, int first) {
-  double gamma_sq = gamma_sq_fixed;
-  if (maxbits) {
-    const double s_max = __longlong_as_double(static_cast<long long>(*maxbits));
-    const double gamma = sqrt(s_max) / 2.0;
-    gamma_sq = (s_max == 0) ? 2.0 : max(2 * gamma * gamma, 1e-10);
-  }
+  const double gamma_sq = frangi_gamma_sq(gamma_sq_fixed, maxbits);
   const F* ev[3] = {l0, l1, l2};
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
     const F r_g = frangi_rg<F>(ev, nd, i);
-    F result;
+    const F result = frangi_value<F>(l0[i], l1[i], nd == 3 ? l2[i] : F(0), nd, r_g, alpha_sq,
+                                     beta_sq, gamma_sq);
+    out[i] = first ? result : frangi_fold(out[i], result);
+  }
+}
+
+// Eigenvalues (ascending by magnitude) and the vesselness in one pass over
+// the Hessian elements (00, 01, 11) or (00, 01, 02, 11, 12, 22): the
+// eigenvalue images are never stored. The same statements as k_eig22 /
+// eig33 + sort3 and k_frangi_inner.
+template <class F>
+__global__ void k_frangi_fused(const F* __restrict__ h0, const F* __restrict__ h1,
+                               const F* __restrict__ h2, const F* __restrict__ h3,
+                               const F* __restrict__ h4, const F* __restrict__ h5, int nd,
+                               int64_t n, double alpha_sq, double beta_sq,
+                               double gamma_sq_fixed, const unsigned long long* maxbits, F* out,
+                               int first) {
+  const double gamma_sq = frangi_gamma_sq(gamma_sq_fixed, maxbits);
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    F lam1, lam2, lam3 = F(0);
     if (nd == 2) {
-      const F lambda1 = l0[i], lambda2 = l1[i];
-      F r_b;
-      r_b = abs(lambda1) / max(lambda2, static_cast<F>(1.0e-10));
-      r_b *= r_b;
-      result = exp(-r_b / beta_sq);
-      result *= 1.0 - exp(-r_g / gamma_sq);
+      // k_eig22's statements with each operation rounded on its own (the
+      // form the compiled k_eig22 was measured to take)
+      F tmp1, tmp2;
+      double m00 = static_cast<double>(h0[i]);
+      double m01 = static_cast<double>(h1[i]);
+      double m11 = static_cast<double>(h2[i]);
+      tmp1 = m01 * m01;
+      tmp1 *= 4;
+      tmp2 = m00 - m11;
+      tmp2 = mul_rn(tmp2, tmp2);
+      tmp2 = add_rn(tmp2, tmp1);
+      tmp2 = sqrt(tmp2);
+      tmp2 /= 2;
+      tmp1 = m00 + m11;
+      tmp1 /= 2;
+      lam1 = tmp1 - tmp2;
+      lam2 = tmp1 + tmp2;
+      if (abs(lam1) > abs(lam2)) {
+        F s = lam1; lam1 = lam2; lam2 = s;
+      }
     } else {
-      const F lambda1 = l0[i], lambda2 = l1[i], lambda3 = l2[i];
-      F r_a, r_b;
-      F lam2 = max(lambda2, static_cast<F>(1.0e-10));
-      F lam3 = max(lambda3, static_cast<F>(1.0e-10));
-      r_a = lam2 / lam3;
-      r_a *= r_a;
-      r_b = (lambda1 * lambda1) / (lam2 * lam3);
-      result = 1.0 - exp(-r_a / alpha_sq);
-      result *= exp(-r_b / beta_sq);
-      result *= 1.0 - exp(-r_g / gamma_sq);
+      // elements (00, 01, 02, 11, 12, 22) = (a, d, f, b, e, c)
+      eig33<F>(h0[i], h3[i], h5[i], h1[i], h4[i], h2[i], lam1, lam2, lam3);
+      sort3(lam1, lam2, lam3, 0, 1);
     }
-    if (first) {
-      out[i] = result;
-    } else {
-      const F prev = out[i];
-      // cupy.maximum: NaN in either operand propagates
-      out[i] = (prev != prev) ? prev : ((result != result) ? result : (prev > result ? prev : result));
-    }
+    F r_g = fma(lam1, lam1, mul_rn(lam2, lam2));
+    if (nd == 3) r_g = fma(lam3, lam3, r_g);
+    const F result = frangi_value<F>(lam1, lam2, lam3, nd, r_g, alpha_sq, beta_sq, gamma_sq);
+    out[i] = first ? result : frangi_fold(out[i], result);
   }
 }
 
@@ -788,3 +851,58 @@ int cimx_frangi_accumulate(const CimxArray* eigs, int ndim, const CimxArray* out
 }
 
 }  // extern "C"
+
+extern "C" int cimx_frangi_hessian_accumulate(const CimxArray* H, int nelems,
+                                              const CimxArray* out, double alpha, double beta,
+                                              double gamma, int first, void* gamma_state,
+                                              void* stream) {
+  using namespace cimx;
+  if (!H || !out || (nelems != 3 && nelems != 6))
+    return fail(CIMX_E_INVALID, "frangi: expected 3 or 6 Hessian element images");
+  const int nd = nelems == 3 ? 2 : 3;
+  const int dt = out->dtype;
+  if (dt != DT_F32 && dt != DT_F64) return fail(CIMX_E_DTYPE, "frangi: float32/float64 only");
+  for (int k = 0; k < nelems; ++k)
+    if (H[k].dtype != dt || !same_shape(&H[k], out) || !contiguous(&H[k]))
+      return fail(CIMX_E_INVALID, "frangi: Hessian images must match the output");
+  if (!contiguous(out)) return fail(CIMX_E_LAYOUT, "not C-contiguous");
+  const int64_t n = numel(out);
+  if (n == 0) return CIMX_OK;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const bool auto_gamma = gamma != gamma;
+  auto* maxbits = static_cast<unsigned long long*>(gamma_state);
+  if (auto_gamma && !maxbits) return fail(CIMX_E_INVALID, "frangi: auto gamma needs a state word");
+  if (auto_gamma && first) {
+    // the first scale's gamma needs the image-wide max of r_g before any
+    // vesselness: eigenvalue images, the max, then the vesselness
+    const size_t bytes = (size_t)n * dtype_size(dt);
+    void* buf = scratch_alloc(bytes * nd, st);
+    if (!buf) return fail(CIMX_E_NOMEM, "scratch allocation for the eigenvalues failed");
+    CimxArray ev[3];
+    for (int k = 0; k < nd; ++k) {
+      ev[k] = *out;
+      ev[k].data = static_cast<char*>(buf) + k * bytes;
+    }
+    int rc = cimx_eigvals_sym(H, nelems, ev, 0, 1, stream);
+    if (!rc) rc = cimx_frangi_accumulate(ev, nd, out, alpha, beta, gamma, first, gamma_state,
+                                         stream);
+    scratch_free(buf, bytes * nd, st);
+    return rc;
+  }
+  const double alpha_sq = 2 * alpha * alpha, beta_sq = 2 * beta * beta;
+  const double gamma_sq = auto_gamma ? 0.0 : 2 * gamma * gamma;
+  const unsigned long long* mb = auto_gamma ? maxbits : nullptr;
+  auto E = [&](int k) { return H[k < nelems ? k : 0].data; };
+  if (dt == DT_F32) {
+    auto P = [&](int k) { return static_cast<const float*>(E(k)); };
+    k_frangi_fused<float><<<grid_for(n), 256, 0, st>>>(P(0), P(1), P(2), P(3), P(4), P(5), nd, n,
+                                                       alpha_sq, beta_sq, gamma_sq, mb,
+                                                       static_cast<float*>(out->data), first);
+  } else {
+    auto P = [&](int k) { return static_cast<const double*>(E(k)); };
+    k_frangi_fused<double><<<grid_for(n), 256, 0, st>>>(P(0), P(1), P(2), P(3), P(4), P(5), nd,
+                                                        n, alpha_sq, beta_sq, gamma_sq, mb,
+                                                        static_cast<double*>(out->data), first);
+  }
+  return cuda_fail(cudaGetLastError(), "frangi launch");
+}

@@ -464,21 +464,60 @@ int cimx_hessian(const CimxArray* in, const CimxArray* elems, int nelems, const 
     const double sq1_2 = 1.0 / std::sqrt(2.0);
     std::vector<double> ss(ndim);
     for (int a = 0; a < ndim; ++a) ss[a] = sq1_2 * sigma[a];
-    for (int a = 0; a < ndim; ++a) {
-      std::vector<int> o(ndim, 0);
-      o[a] = 1;
-      if ((rc = cimx_gaussian_nd(&img, &grads[a], ss.data(), o.data(), nullptr, modes.data(),
-                                 nullptr, ndim, truncate, cval, CIMX_ALGO_AUTO, lib_flags,
-                                 stream)))
+    if (ndim == 1) {
+      std::vector<int> o(1, 1);
+      if ((rc = cimx_gaussian_nd(&img, &grads[0], ss.data(), o.data(), nullptr, modes.data(),
+                                 nullptr, 1, truncate, cval, CIMX_ALGO_AUTO, lib_flags, stream)))
         return rc;
+      return cimx_gaussian_nd(&grads[0], &elems[0], ss.data(), o.data(), nullptr, modes.data(),
+                              nullptr, 1, truncate, cval, CIMX_ALGO_AUTO, lib_flags, stream);
     }
-    for (int i = 0; i < nelems; ++i) {
-      std::vector<int> o(ndim, 0);
-      o[pairs[i].second] = 1;
-      if ((rc = cimx_gaussian_nd(&grads[pairs[i].first], &elems[i], ss.data(), o.data(),
-                                 nullptr, modes.data(), nullptr, ndim, truncate, cval,
-                                 CIMX_ALGO_AUTO, lib_flags, stream)))
-        return rc;
+    // Every chain runs its axis-0 pass first, and chains share it: the
+    // gradients along axes >= 1 all start with the order-0 pass on the image,
+    // H[a0][a1] for a1 >= 1 all start with the order-0 pass on gradient a0.
+    // Each shared pass runs once into scratch and the rest of each chain is a
+    // call over the remaining axes: the same passes in the same order, so the
+    // results are bit-identical.
+    std::vector<int> rest_axes, rest_modes(ndim - 1, mode);
+    std::vector<double> rest_sigma;
+    for (int a = 1; a < ndim; ++a) {
+      rest_axes.push_back(a);
+      rest_sigma.push_back(ss[a]);
+    }
+    void* lp = scratch.get(2 * fb);
+    if (!lp) return fail(CIMX_E_NOMEM, "scratch allocation for the shared passes failed");
+    CimxArray lead[2] = {dense_like(in, lp, F), dense_like(in, static_cast<char*>(lp) + fb, F)};
+    const int axis0[1] = {0};
+    // lead[o] = the axis-0 pass of order o on `src`
+    auto lead_pass = [&](const CimxArray* src, int o, const CimxArray* dst) {
+      const int ord[1] = {o};
+      return cimx_gaussian_nd(src, dst, ss.data(), ord, nullptr, modes.data(), axis0, 1,
+                              truncate, cval, CIMX_ALGO_AUTO, lib_flags, stream);
+    };
+    // the rest of a chain of orders e_b over axes 1..ndim-1
+    auto rest = [&](const CimxArray* src, int b, const CimxArray* dst) {
+      std::vector<int> ord(ndim - 1, 0);
+      if (b >= 1) ord[b - 1] = 1;
+      return cimx_gaussian_nd(src, dst, rest_sigma.data(), ord.data(), nullptr,
+                              rest_modes.data(), rest_axes.data(), ndim - 1, truncate, cval,
+                              CIMX_ALGO_AUTO, lib_flags, stream);
+    };
+    if ((rc = lead_pass(&img, 1, &lead[1])) || (rc = rest(&lead[1], 0, &grads[0]))) return rc;
+    if ((rc = lead_pass(&img, 0, &lead[0]))) return rc;
+    for (int a = 1; a < ndim; ++a)
+      if ((rc = rest(&lead[0], a, &grads[a]))) return rc;
+    // H elements grouped by their gradient; each group's two axis-0 passes once
+    for (int a0 = 0; a0 < ndim; ++a0) {
+      bool done[2] = {false, false};
+      for (int i = 0; i < nelems; ++i) {
+        if (pairs[i].first != a0) continue;
+        const int b = pairs[i].second, o0 = b == 0 ? 1 : 0;
+        if (!done[o0]) {
+          if ((rc = lead_pass(&grads[a0], o0, &lead[o0]))) return rc;
+          done[o0] = true;
+        }
+        if ((rc = rest(&lead[o0], b, &elems[i]))) return rc;
+      }
     }
     return CIMX_OK;
   }
@@ -548,7 +587,8 @@ int cimx_ridge_filter(const CimxArray* in, const CimxArray* out, int kind, const
     if (!(p = scratch.get(fb))) return fail(CIMX_E_NOMEM, "scratch allocation failed");
     H[i] = dense_like(in, p, F);
   }
-  for (int i = 0; i < ndim; ++i) {
+  // eigenvalue images for meijering and sato (frangi's stay in registers)
+  for (int i = 0; i < ndim && kind != CIMX_RIDGE_FRANGI && kind != CIMX_RIDGE_HESSIAN; ++i) {
     if (!(p = scratch.get(fb))) return fail(CIMX_E_NOMEM, "scratch allocation failed");
     ev[i] = dense_like(in, p, F);
   }
@@ -564,14 +604,15 @@ int cimx_ridge_filter(const CimxArray* in, const CimxArray* out, int kind, const
     if ((rc = cimx_hessian(&img, H.data(), nelems, sig.data(), mode, cval, 1, 0, lib_flags,
                            stream)))
       return rc;
-    // frangi sorts ascending by magnitude (ridges.py:433-435); the others
-    // take hessian_matrix_eigvals, descending (corner.py:824-858)
-    if ((rc = cimx_eigvals_sym(H.data(), nelems, ev.data(), frangi_like ? 0 : 1,
-                               frangi_like ? 1 : 0, stream)))
+    // meijering and sato take hessian_matrix_eigvals, descending
+    // (corner.py:824-858); frangi's eigenvalues are computed inside its
+    // epilogue kernel
+    if (!frangi_like && (rc = cimx_eigvals_sym(H.data(), nelems, ev.data(), 1, 0, stream)))
       return rc;
     const int first = s == 0 ? 1 : 0;
     if (frangi_like)
-      rc = cimx_frangi_accumulate(ev.data(), ndim, out, alpha, beta, gamma, first, state, stream);
+      rc = cimx_frangi_hessian_accumulate(H.data(), nelems, out, alpha, beta, gamma, first, state,
+                                          stream);
     else if (kind == CIMX_RIDGE_MEIJERING)
       rc = cimx_meijering_accumulate(ev.data(), ndim, out, alpha, first, state, stream);
     else

@@ -50,11 +50,39 @@ def _hessian_matrix_with_gaussian(image, sigma=1, mode="reflect", cval=0, order=
         return ndi.gaussian_filter(img, sigma_scaled, order=o, mode=mode, cval=cval,
                                    truncate=truncate, algorithm=algorithm)
 
-    gradients = [g(image, orders[d]) for d in range(ndim)]
-    axes = range(ndim)
+    axes = list(range(ndim))
     if order == "xy":
-        axes = reversed(axes)
-    return [g(gradients[a0], orders[a1]) for a0, a1 in combinations_with_replacement(axes, 2)]
+        axes = axes[::-1]
+    if ndim < 2:
+        gradients = [g(image, orders[d]) for d in range(ndim)]
+        return [g(gradients[a0], orders[a1]) for a0, a1 in combinations_with_replacement(axes, 2)]
+
+    # Every chain runs its axis-0 pass first and most chains share it: the
+    # gradients along axes >= 1 all start with the order-0 pass on the image,
+    # and H[a0, a1] for a1 >= 1 all start with the order-0 pass on gradient
+    # a0. Each shared pass runs once (a 1-pass call) and the rest of each
+    # chain is a call over the remaining axes: the same passes in the same
+    # order, so the results are bit-identical (6 axis-0 passes instead of 9
+    # in 3-D).
+    rest = tuple(range(1, ndim))
+
+    def part(img, o, ax):
+        return ndi.gaussian_filter(img, [sigma_scaled[a] for a in ax],
+                                   order=[o[a] for a in ax], mode=mode, cval=cval,
+                                   truncate=truncate, axes=ax, algorithm=algorithm)
+
+    lead = {}
+
+    def lead_pass(key, img, o0):
+        if (key, o0) not in lead:
+            lead[(key, o0)] = part(img, [o0] + [0] * (ndim - 1), (0,))
+        return lead[(key, o0)]
+
+    gradients = [part(lead_pass("image", image, orders[d][0]), orders[d], rest)
+                 for d in range(ndim)]
+    lead.clear()
+    return [part(lead_pass(a0, gradients[a0], orders[a1][0]), orders[a1], rest)
+            for a0, a1 in combinations_with_replacement(axes, 2)]
 
 
 def _gradient(f, axis):

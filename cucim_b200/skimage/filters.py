@@ -296,13 +296,16 @@ def frangi(image, sigmas=range(1, 10, 2), scale_range=None, scale_step=None, alp
     g = float("nan") if gamma is None else float(gamma)
     a_out = _arrays.to_cimx(out)
     for i, sigma in enumerate(sigmas):
-        H = _hessian_matrix_with_gaussian(image, sigma, mode=mode, cval=cval, algorithm=algorithm)
-        ev = _arrays.as_tensor(symmetric_compute_eigenvalues(H, sort="ascending", abs_sort=True))
-        eigs = (_lib.CimxArray * ndim)(*[_arrays.to_cimx(ev[k]) for k in range(ndim)])
-        rc = _lib.lib.cimx_frangi_accumulate(eigs, ndim, ctypes.byref(a_out), float(alpha),
-                                             float(beta), g, 1 if i == 0 else 0,
-                                             ctypes.c_void_p(state.data_ptr()),
-                                             _arrays.stream_of(out))
+        H = [_arrays.as_tensor(h).contiguous() for h in
+             _hessian_matrix_with_gaussian(image, sigma, mode=mode, cval=cval,
+                                           algorithm=algorithm)]
+        # eigenvalues and vesselness in one pass over the Hessian elements
+        hs = (_lib.CimxArray * len(H))(*[_arrays.to_cimx(h) for h in H])
+        rc = _lib.lib.cimx_frangi_hessian_accumulate(hs, len(H), ctypes.byref(a_out),
+                                                     float(alpha), float(beta), g,
+                                                     1 if i == 0 else 0,
+                                                     ctypes.c_void_p(state.data_ptr()),
+                                                     _arrays.stream_of(out))
         _lib.check(rc, "frangi")
     return _arrays.wrap_like(image, out)
 

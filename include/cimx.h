@@ -467,6 +467,19 @@ CIMX_API int cimx_corner_response(int kind, const CimxArray* inputs, int ninputs
                                   const CimxArray* out, const CimxArray* out2, double param,
                                   void* stream);
 
+/* One scale of frangi from the Hessian elements themselves, (00, 01, 11) or
+ * (00, 01, 02, 11, 12, 22): the eigenvalues (ascending by magnitude) and the
+ * vesselness in one kernel, folded into `out` like cimx_frangi_accumulate,
+ * without storing the eigenvalue images. For the first scale with the
+ * automatic gamma (gamma NaN, first != 0), whose gamma needs the image-wide
+ * maximum first, the eigenvalues go through scratch memory as in
+ * cimx_eigvals_sym + cimx_frangi_accumulate. Results are bit-identical to
+ * that pair. filters/ridges.py:425-475. */
+CIMX_API int cimx_frangi_hessian_accumulate(const CimxArray* H, int nelems,
+                                            const CimxArray* out, double alpha, double beta,
+                                            double gamma, int first, void* gamma_state,
+                                            void* stream);
+
 /* One tile of a batch for cimx_batch_gray_gauss_sobel. */
 typedef struct CimxBatchTile {
   const uint8_t* rgb;   /* device: height x width x 3 uint8, C-contiguous */

@@ -150,3 +150,40 @@ def test_linearity(filters, shape):
         np.testing.assert_allclose(host(f(dev(1 * a_white), black_ridges=False, **kw)),
                                    host(f(dev(10 * a_white), black_ridges=False, **kw)),
                                    atol=1e-3, err_msg=name)
+
+
+@pytest.mark.parametrize("shape", [(36, 41), (14, 17, 19)])
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+@pytest.mark.parametrize("gamma", [None, 0.7])
+def test_fused_frangi_epilogue_equals_two_step(filters, shape, dtype, gamma):
+    """cimx_frangi_hessian_accumulate (eigenvalues and vesselness in one
+    kernel) against cimx_eigvals_sym + cimx_frangi_accumulate, bit for bit,
+    over three scales (the first with the automatic gamma goes through
+    the eigenvalue images, the others through the fused kernel)."""
+    import ctypes
+
+    from cucim_b200 import _arrays, _lib
+    from cucim_b200.skimage.feature import _hessian_matrix_with_gaussian
+
+    x = dev(np.random.default_rng(12).random(shape).astype(dtype))
+    nd = len(shape)
+    g = float("nan") if gamma is None else gamma
+    outs = [torch.empty_like(x), torch.empty_like(x)]
+    states = [torch.zeros(2, dtype=torch.int64, device="cuda") for _ in range(2)]
+    for i, sigma in enumerate([1.0, 2.0, 3.0]):
+        H = [h.contiguous() for h in _hessian_matrix_with_gaussian(x, sigma)]
+        hs = (_lib.CimxArray * len(H))(*[_arrays.to_cimx(h) for h in H])
+        a0 = _arrays.to_cimx(outs[0])
+        assert _lib.lib.cimx_frangi_hessian_accumulate(
+            hs, len(H), ctypes.byref(a0), 0.5, 0.5, g, int(i == 0),
+            ctypes.c_void_p(states[0].data_ptr()), None) == 0, _lib.last_error()
+        ev = torch.empty((nd,) + tuple(shape), dtype=x.dtype, device="cuda")
+        evs = (_lib.CimxArray * nd)(*[_arrays.to_cimx(ev[k]) for k in range(nd)])
+        assert _lib.lib.cimx_eigvals_sym(hs, len(H), evs, 0, 1, None) == 0
+        a1 = _arrays.to_cimx(outs[1])
+        assert _lib.lib.cimx_frangi_accumulate(evs, nd, ctypes.byref(a1), 0.5, 0.5, g,
+                                               int(i == 0),
+                                               ctypes.c_void_p(states[1].data_ptr()),
+                                               None) == 0
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(host(outs[0]), host(outs[1]))
