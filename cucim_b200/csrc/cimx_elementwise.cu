@@ -872,9 +872,13 @@ extern "C" int cimx_frangi_hessian_accumulate(const CimxArray* H, int nelems,
   const bool auto_gamma = gamma != gamma;
   auto* maxbits = static_cast<unsigned long long*>(gamma_state);
   if (auto_gamma && !maxbits) return fail(CIMX_E_INVALID, "frangi: auto gamma needs a state word");
-  if (auto_gamma && first) {
+  if ((auto_gamma && first) || dt == DT_F64) {
     // the first scale's gamma needs the image-wide max of r_g before any
-    // vesselness: eigenvalue images, the max, then the vesselness
+    // vesselness: eigenvalue images, the max, then the vesselness. float64
+    // takes this path on every scale: its eigenvalues are not rounded to
+    // float, so the last bit of the float64 solve would show how the
+    // compiler contracted it inside the fused kernel, where the standalone
+    // eigenvalue kernel is compiled like cuCIM's own
     const size_t bytes = (size_t)n * dtype_size(dt);
     void* buf = scratch_alloc(bytes * nd, st);
     if (!buf) return fail(CIMX_E_NOMEM, "scratch allocation for the eigenvalues failed");

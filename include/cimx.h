@@ -472,9 +472,9 @@ CIMX_API int cimx_corner_response(int kind, const CimxArray* inputs, int ninputs
  * vesselness in one kernel, folded into `out` like cimx_frangi_accumulate,
  * without storing the eigenvalue images. For the first scale with the
  * automatic gamma (gamma NaN, first != 0), whose gamma needs the image-wide
- * maximum first, the eigenvalues go through scratch memory as in
- * cimx_eigvals_sym + cimx_frangi_accumulate. Results are bit-identical to
- * that pair. filters/ridges.py:425-475. */
+ * maximum first, and for float64 images on every scale, the eigenvalues go
+ * through scratch memory as in cimx_eigvals_sym + cimx_frangi_accumulate.
+ * Results are bit-identical to that pair. filters/ridges.py:425-475. */
 CIMX_API int cimx_frangi_hessian_accumulate(const CimxArray* H, int nelems,
                                             const CimxArray* out, double alpha, double beta,
                                             double gamma, int first, void* gamma_state,
