@@ -4,9 +4,9 @@ tests/golden/known_answers.json.
 cuCIM cannot be imported here (it needs CuPy), so its files are read as
 text: each entry below names the file and line range that holds a literal
 array, which is parsed with ast.literal_eval. Run from the repository root
-with the cuCIM sources at REF (default /root/reference):
+with the root of a cuCIM source checkout as the only argument:
 
-    python tests/golden/make_known_answers.py [REF]
+    python tests/golden/make_known_answers.py <cucim source root>
 """
 
 import ast
@@ -15,7 +15,9 @@ import os
 import re
 import sys
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) != 2:
+    sys.exit("usage: python tests/golden/make_known_answers.py <cucim source root>")
+REF = sys.argv[1]
 SK = "python/cucim/src/cucim/skimage"
 
 # (key, file, first line, last line): the literal arrays inside that range,
