@@ -68,6 +68,8 @@ class CimxBatchTile(ctypes.Structure):
         ("ntaps", ctypes.c_int32),
         ("taps_offset", ctypes.c_int32),
         ("first_block", ctypes.c_int64),
+        ("rgb_pitch", ctypes.c_int64),
+        ("out_pitch", ctypes.c_int64),
     ]
 
 

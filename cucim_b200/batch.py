@@ -9,9 +9,15 @@ this library; cuCIM runs `color.rgb2gray`, `filters.gaussian` and
     batch.outputs                            # float32 tiles, bit-identical to
                                              # sobel(gaussian(rgb2gray(t), s))
 
-Each tile is an (H, W, 3) uint8 CUDA tensor (C-contiguous); its output is
-(H, W) float32. The gaussian uses mode 'nearest' and truncate 4 (the
-defaults of `skimage.filters.gaussian`), the sobel mode 'reflect'.
+Each tile is an (H, W, 3) uint8 CUDA tensor whose pixels are contiguous
+within a row (a C-contiguous tile, or a region view of a larger slide: rows
+may be any pitch apart); its output is (H, W) float32 (C-contiguous or a
+region view). `TileBatch.from_regions(slide, regions, sigmas)` builds the
+batch straight from regions of a whole-slide image held on the device, the
+way a slide reader's read_region results feed it, without copying tiles.
+The gaussian uses mode 'nearest' and truncate 4 (the defaults of
+`skimage.filters.gaussian`), the sobel mode 'reflect'; every tile is
+filtered as an image of its own, exactly as the per-tile calls would.
 """
 
 import ctypes
@@ -56,8 +62,10 @@ class TileBatch:
         self.device = rgb_tiles[0].device if rgb_tiles else torch.device("cuda")
         self.tiles = [_arrays.as_tensor(t) for t in rgb_tiles]
         for t in self.tiles:
-            if t.dtype != torch.uint8 or t.dim() != 3 or t.shape[-1] != 3 or not t.is_contiguous():
-                raise ValueError("tiles must be C-contiguous (H, W, 3) uint8 CUDA tensors")
+            if (t.dtype != torch.uint8 or t.dim() != 3 or t.shape[-1] != 3
+                    or t.stride(2) != 1 or t.stride(1) != 3 or t.stride(0) < 3 * t.shape[1]):
+                raise ValueError("tiles must be (H, W, 3) uint8 CUDA tensors with contiguous "
+                                 "pixels in each row")
         if outputs is None:
             outputs = [torch.empty(t.shape[:2], dtype=torch.float32, device=t.device)
                        for t in self.tiles]
@@ -83,10 +91,11 @@ class TileBatch:
         first = 0
         for i, (t, o) in enumerate(zip(self.tiles, outputs)):
             h, w = int(t.shape[0]), int(t.shape[1])
-            if tuple(o.shape) != (h, w) or o.dtype != torch.float32 or not o.is_contiguous():
-                raise ValueError("outputs must be C-contiguous (H, W) float32 tensors")
+            if (tuple(o.shape) != (h, w) or o.dtype != torch.float32 or o.stride(1) != 1
+                    or o.stride(0) < w):
+                raise ValueError("outputs must be (H, W) float32 tensors with contiguous rows")
             table[i] = _lib.CimxBatchTile(t.data_ptr(), o.data_ptr(), h, w, ntaps[i], offsets[i],
-                                          first)
+                                          first, t.stride(0), o.stride(0))
             first += ((h + BLOCK - 1) // BLOCK) * ((w + BLOCK - 1) // BLOCK)
         self.nblocks = first
         raw = np.frombuffer(bytes(table), dtype=np.uint8).copy()
@@ -95,6 +104,31 @@ class TileBatch:
         self._edge = (ctypes.c_float * 3)(*ew.tolist())
         self._smooth = (ctypes.c_float * 3)(*sw.tolist())
         self.npixels = sum(int(t.shape[0]) * int(t.shape[1]) for t in self.tiles)
+
+    @classmethod
+    def from_regions(cls, slide, regions, sigmas, out_slide=None, truncate=4.0):
+        """A batch over regions (y, x, height, width) of one (H, W, 3) uint8
+        slide on the device: the tiles are views into the slide (no copies).
+        With `out_slide` ((H, W) float32), each region's result is written
+        into the same region of it (regions must then not overlap); else
+        every region gets its own (height, width) output."""
+        import torch
+
+        s = _arrays.as_tensor(slide)
+        if s.dim() != 3 or s.shape[-1] != 3 or s.dtype != torch.uint8:
+            raise ValueError("the slide must be an (H, W, 3) uint8 array")
+        H, W = int(s.shape[0]), int(s.shape[1])
+        tiles, outs = [], None if out_slide is None else []
+        o_all = None if out_slide is None else _arrays.as_tensor(out_slide)
+        if o_all is not None and tuple(o_all.shape) != (H, W):
+            raise ValueError("out_slide must have the slide's (H, W) shape")
+        for (y, x, h, w) in regions:
+            if not (0 <= y and 0 <= x and h >= 1 and w >= 1 and y + h <= H and x + w <= W):
+                raise ValueError(f"region {(y, x, h, w)} is outside the {H} x {W} slide")
+            tiles.append(s[y:y + h, x:x + w])
+            if o_all is not None:
+                outs.append(o_all[y:y + h, x:x + w])
+        return cls(tiles, sigmas, outputs=outs, truncate=truncate)
 
     def run(self, stream=None):
         import torch

@@ -188,7 +188,7 @@ using namespace cimx;
 
 extern "C" {
 
-int cimx_abi_version(void) { return 100; }
+int cimx_abi_version(void) { return 101; }
 
 const char* cimx_last_error_string(void) { return g_last_error.c_str(); }
 

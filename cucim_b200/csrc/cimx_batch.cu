@@ -32,7 +32,7 @@ namespace {
 constexpr int kBT = 64;          // output block side
 constexpr int kBThreads = 256;
 constexpr int kBMaxTaps = 129;   // radius <= 64
-static_assert(sizeof(CimxBatchTile) == 40, "CimxBatchTile layout is part of the ABI");
+static_assert(sizeof(CimxBatchTile) == 56, "CimxBatchTile layout is part of the ABI");
 
 struct BatchArgs {
   const CimxBatchTile* tiles;
@@ -80,6 +80,9 @@ __global__ void __launch_bounds__(kBThreads, 2) k_batch_gray_gauss_sobel(const B
     __syncthreads();
     const CimxBatchTile t = a.tiles[s_tile];
     const int H = t.height, W = t.width;
+    // row pitches: a tile may be a region of a larger slide (0 = packed)
+    const long long in_pitch = t.rgb_pitch > 0 ? t.rgb_pitch : 3LL * W;
+    const long long out_pitch = t.out_pitch > 0 ? t.out_pitch : W;
     const int nbx = (W + kBT - 1) / kBT;
     const long long j = g - t.first_block;
     // a block index outside the tile (inconsistent table) is skipped; the
@@ -99,7 +102,7 @@ __global__ void __launch_bounds__(kBThreads, 2) k_batch_gray_gauss_sobel(const B
     for (int idx = tid; idx < GR * GC; idx += kBThreads) {
       const int gr = idx / GC, c = idx - gr * GC;
       const int gy = nearest_idx(y0 - 1 - r + gr, H), gx = nearest_idx(x0 - 1 - r + c, W);
-      G[gr * gcs + c] = luma_u8(t.rgb + (static_cast<long long>(gy) * W + gx) * 3);
+      G[gr * gcs + c] = luma_u8(t.rgb + static_cast<long long>(gy) * in_pitch + gx * 3LL);
     }
     __syncthreads();
 
@@ -164,7 +167,7 @@ __global__ void __launch_bounds__(kBThreads, 2) k_batch_gray_gauss_sobel(const B
       d1 = fmaf(e1[kBT], a.smooth[1], d1);
       d1 = fmaf(e1[2 * kBT], a.smooth[2], d1);
       const float m = __fadd_rn(__fmul_rn(d0, d0), __fmul_rn(d1, d1));
-      t.out[static_cast<long long>(y0 + y) * W + x0 + x] = sqrtf(m);
+      t.out[static_cast<long long>(y0 + y) * out_pitch + x0 + x] = sqrtf(m);
     }
     __syncthreads();  // shared buffers are reused by the next block
   }

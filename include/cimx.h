@@ -117,7 +117,7 @@ enum {
 };
 
 /* Version of this ABI (major*100 + minor). */
-CIMX_API int cimx_abi_version(void);
+CIMX_API int cimx_abi_version(void);  /* 101: CimxBatchTile row pitches */
 
 /* Description of the last error raised on the calling thread. */
 CIMX_API const char* cimx_last_error_string(void);
@@ -482,13 +482,16 @@ CIMX_API int cimx_frangi_hessian_accumulate(const CimxArray* H, int nelems,
 
 /* One tile of a batch for cimx_batch_gray_gauss_sobel. */
 typedef struct CimxBatchTile {
-  const uint8_t* rgb;   /* device: height x width x 3 uint8, C-contiguous */
-  float* out;           /* device: height x width float32, C-contiguous */
+  const uint8_t* rgb;   /* device: height rows of width x 3 uint8 (pixels interleaved) */
+  float* out;           /* device: height rows of width float32 */
   int32_t height, width;
   int32_t ntaps;        /* gaussian taps of this tile (odd, <= max_taps) */
   int32_t taps_offset;  /* index of the tile's first tap in `taps` */
   int64_t first_block;  /* index of the tile's first 64 x 64 output block; tiles in
                            ascending order, the first at 0 */
+  int64_t rgb_pitch;    /* bytes from one rgb row to the next (0: 3 * width); a region
+                           of a larger slide image passes the slide's row pitch */
+  int64_t out_pitch;    /* float32 elements from one output row to the next (0: width) */
 } CimxBatchTile;
 
 /* For every tile of a batch: rgb2gray (color/colorconv.py:1038-1095 with the

@@ -74,3 +74,37 @@ def test_batch_rejects_long_filters(cuda):
     tiles = _tiles([(16, 16)], 6)
     with pytest.raises(ValueError):
         batch.TileBatch(tiles, [20.0])  # 161 taps
+
+
+def test_batch_from_slide_regions(cuda):
+    """Tiles taken as regions of one slide image on the device (views with
+    the slide's row pitch, no copies), written into their own outputs and
+    into the matching regions of a slide-sized output: bit-identical to the
+    per-tile calls on copies of the regions."""
+    from cucim_b200 import batch
+
+    slide = _tiles([(700, 900)], 8)[0]
+    regions = [(0, 0, 64, 64), (10, 600, 300, 299), (650, 850, 50, 50), (100, 0, 1, 900),
+               (333, 444, 77, 3)]
+    sigmas = [1.0, 3.3, 0.6, 2.0, 7.5]
+    b = batch.TileBatch.from_regions(slide, regions, sigmas)
+    got = b.run()
+    copies = [slide[y:y + h, x:x + w].contiguous() for y, x, h, w in regions]
+    ref = batch.gray_gauss_sobel_per_tile(copies, sigmas)
+    torch.cuda.synchronize()
+    for g, r in zip(got, ref):
+        assert torch.equal(g, r)
+    # into one slide-sized output (non-overlapping regions)
+    out_slide = torch.full((700, 900), -1.0, device="cuda")
+    regions2 = [(0, 0, 64, 64), (10, 600, 300, 299), (650, 850, 50, 50)]
+    b2 = batch.TileBatch.from_regions(slide, regions2, sigmas[:3], out_slide=out_slide)
+    b2.run()
+    torch.cuda.synchronize()
+    for (y, x, h, w), r in zip(regions2, ref[:3]):
+        assert torch.equal(out_slide[y:y + h, x:x + w], r)
+    untouched = torch.ones_like(out_slide, dtype=torch.bool)
+    for y, x, h, w in regions2:
+        untouched[y:y + h, x:x + w] = False
+    assert bool((out_slide[untouched] == -1.0).all())
+    with pytest.raises(ValueError):
+        batch.TileBatch.from_regions(slide, [(690, 0, 20, 20)], [1.0])

@@ -30,7 +30,7 @@ def test_every_declared_symbol_is_exported():
 
 
 def test_abi_version():
-    assert _lib.lib.cimx_abi_version() == 100
+    assert _lib.lib.cimx_abi_version() == 101
 
 
 def _arr(shape, dtype, ptr=0x1000, strides=None):
