@@ -76,8 +76,18 @@ def empty(shape, dtype, device):
     return torch.empty(tuple(shape), dtype=torch_dtype(dtype), device=device)
 
 
+# CimxArray structs by (pointer, dtype, shape, strides): building a ctypes
+# struct costs more than the lookup, and filters are called on the same
+# buffers over and over. The structs are only read by the library.
+_CIMX_CACHE = {}
+
+
 def to_cimx(t):
     """CimxArray describing a C-contiguous CUDA tensor."""
+    key = (t.data_ptr(), t.dtype, t.shape, t.stride())
+    a = _CIMX_CACHE.get(key)
+    if a is not None:
+        return a
     if t.dim() > _lib.MAX_NDIM:
         raise NotImplementedError(f"ndim > {_lib.MAX_NDIM} is not supported")
     a = _lib.CimxArray()
@@ -88,10 +98,19 @@ def to_cimx(t):
     for d in range(t.dim()):
         a.shape[d] = t.shape[d]
         a.strides[d] = t.stride(d) * es
+    if len(_CIMX_CACHE) >= 4096:
+        _CIMX_CACHE.clear()
+    _CIMX_CACHE[key] = a
     return a
 
 
+_RAW_STREAM = getattr(torch._C, "_cuda_getCurrentRawStream", None)
+
+
 def stream_of(t):
+    """The current torch stream of `t`'s device, as a raw cudaStream_t."""
+    if _RAW_STREAM is not None:
+        return _RAW_STREAM(t.get_device())
     return torch.cuda.current_stream(t.device).cuda_stream
 
 
@@ -101,6 +120,9 @@ def shares_memory(a, b):
         return False
     if a.device != b.device:
         return False
+    if a.is_contiguous() and b.is_contiguous():
+        a0, b0 = a.data_ptr(), b.data_ptr()
+        return a0 < b0 + b.numel() * b.element_size() and b0 < a0 + a.numel() * a.element_size()
 
     def bounds(t):
         lo = hi = t.data_ptr()

@@ -135,6 +135,12 @@ def schedule(lib_flags):
 
 def _hashable(obj):
     """`obj` with lists turned into tuples, or None when it cannot be a key."""
+    if not isinstance(obj, list):
+        try:  # scalars and tuples of scalars: already a key
+            hash(obj)
+            return obj
+        except TypeError:
+            pass
     if isinstance(obj, (list, tuple)):
         items = tuple(_hashable(o) for o in obj)
         return None if any(i is None and o is not None for i, o in zip(items, obj)) else items
