@@ -1,7 +1,6 @@
 // cimx_fast_f32.cu — instantiations of the fast kernels (cimx_fast.cuh) for
 // float input. Split by input dtype so the kernels compile in parallel.
 #include "cimx_fast.cuh"
-#include "cimx_slabw.cuh"
 #include "cimx_vol.cuh"
 
 namespace cimx {
@@ -17,14 +16,8 @@ int launch_stream_f32(const PassDesc& d, const float* w, int K, int anchor,
 
 int launch_slab_f32(SlabArgs& a, int tout, cudaStream_t st) {
   using namespace fast;
-  if (tout != DT_F32) return CIMX_FUSED_DECLINED;
-  // the row stream keeps the short (3 / 5-tap) passes it was measured
-  // fastest for; the persistent warp-specialised kernel takes the others
-  if (a.has_y && !rowstream_fits<float, float>(a)) {
-    const int rc = launch_slabw(a, st);
-    if (rc != CIMX_FUSED_DECLINED) return rc;
-  }
-  return launch_slab_td<float, float>(a, st);
+  if (tout == DT_F32) return launch_slab_td<float, float>(a, st);
+  return CIMX_FUSED_DECLINED;
 }
 
 int launch_vol_f32(const VolArgs& v, int tout, cudaStream_t st) {

@@ -226,7 +226,6 @@ int try_fused(const CimxArray* in, const CimxArray* out, PassDesc* ds, int npass
   if (rc == CIMX_OK && !tail.empty()) {
     SlabArgs a{};
     a.no_rowstream = (lib_flags & CIMX_L_NO_ROWSTREAM) ? 1 : 0;
-    a.no_slabw = (lib_flags & CIMX_L_NO_SLABW) ? 1 : 0;
     a.in = src;
     a.out = dst_of(j++);
     a.X = in->shape[nd - 1];

@@ -30,7 +30,6 @@ struct SlabArgs {
   int has_y, has_x;
   int* status;  // device status word for bounded waits
   int no_rowstream;  // CIMX_L_NO_ROWSTREAM: always the slab kernel
-  int no_slabw;      // CIMX_L_NO_SLABW: the one-tile-per-CTA slab kernel
   SlabPass py, px;
 };
 

@@ -91,8 +91,6 @@ enum {
   CIMX_L_NO_TUNE = 1 << 7,      /* this call neither consults nor fills the tuning table */
   CIMX_L_ZCHUNK_SHIFT = 8,      /* bits 8-9: volume-kernel z chunk, 0 = automatic,
                                    1/2/3 = 32/64/128 slices */
-  CIMX_L_NO_SLABW = 1 << 10,    /* float32 (y, x) passes on the one-tile-per-CTA slab kernel,
-                                   not the persistent warp-specialised one */
 };
 
 /* One 1-D correlation pass of a separable filter. */
