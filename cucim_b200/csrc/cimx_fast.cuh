@@ -313,12 +313,7 @@ template <class T, int KB>
 struct Geom {
   static constexpr bool F32 = sizeof(T) == 4;
   static constexpr int RY = kSlabTY + KB;         // staged rows
-  // output columns per tile: 128, narrowed for longer taps so that the staged
-  // width stays 152 columns: 77 y-pass column pairs x 4 row groups fit 320
-  // threads, which keeps three CTAs per SM resident (with 128 columns, 32-48
-  // taps need 352-384 threads and the register budget allows only two)
-  static constexpr int TX = KB <= 24 ? kSlabTX : 152 - KB;
-  static constexpr int RX = TX + KB;              // staged columns (even)
+  static constexpr int RX = kSlabTX + KB;         // staged columns (even)
   static constexpr int NPAIR = RX / 2 + 1;        // y-pass column pairs (one spare for sh)
   static constexpr int RXS = RX + 2;              // s_in row stride (floats)
   static constexpr int RXQ = pad8(RX + 2);        // s_mid row-pair stride (float2)
@@ -499,7 +494,7 @@ __global__ void __launch_bounds__(Geom<T, KB>::NT, Geom<T, KB>::MINB) k_slab(con
   const float cx = a.has_x ? fill_value<float>(a.px.cval, a.px.cval_as_input, a.px.dt) : 0.f;
   // grid = (tiles_x, tiles_y, slabs); slabs beyond the grid's z extent are
   // visited by striding, the mbarrier phase flipping once per slab
-  const long long y0 = (long long)blockIdx.y * kSlabTY, x0 = (long long)blockIdx.x * G::TX;
+  const long long y0 = (long long)blockIdx.y * kSlabTY, x0 = (long long)blockIdx.x * kSlabTX;
   const long long ys = y0 - ay, xst = x0 - ax;
   const long long xs = floor_div(xst, G::VE) * G::VE;  // 16-byte aligned TMA start column
   const int off = static_cast<int>(xst - xs);
@@ -653,9 +648,9 @@ __global__ void __launch_bounds__(Geom<T, KB>::NT, Geom<T, KB>::MINB) k_slab(con
         for (int p = 0; p < P; ++p) {
           const long long yy = y0 + rg + p;
           if (yy >= a.Y) continue;
-          if (c0 >= 0 && c0 < G::TX && x0 + c0 < a.X)
+          if (c0 >= 0 && c0 < kSlabTX && x0 + c0 < a.X)
             out[yy * a.X + x0 + c0] = narrow_cast<D>(lo2(acc[p]));
-          if (c0 + 1 >= 0 && c0 + 1 < G::TX && x0 + c0 + 1 < a.X)
+          if (c0 + 1 >= 0 && c0 + 1 < kSlabTX && x0 + c0 + 1 < a.X)
             out[yy * a.X + x0 + c0 + 1] = narrow_cast<D>(hi2(acc[p]));
         }
       }
@@ -667,7 +662,7 @@ __global__ void __launch_bounds__(Geom<T, KB>::NT, Geom<T, KB>::MINB) k_slab(con
     // 3. x pass: one row pair x P consecutive outputs per item; output column
     //    g + q reads s_mid column g + q + sh, and since g is a multiple of 8,
     //    pad8(g + q + sh) = pad8(g) + pad8(q + sh)
-    constexpr int gpr = G::TX / P;
+    constexpr int gpr = kSlabTX / P;
     for (int item = threadIdx.x; item < (kSlabTY / 2) * gpr; item += blockDim.x) {
       const int rp = item / gpr;
       const int g = (item % gpr) * P;
@@ -714,7 +709,7 @@ int launch_slab_kb(SlabArgs& a, cudaStream_t st) {
     cudaFuncSetAttribute(k_slab<T, D, KB, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          kMaxSmem);
   });
-  a.tiles_x = (a.X + G::TX - 1) / G::TX;
+  a.tiles_x = (a.X + kSlabTX - 1) / kSlabTX;
   a.tiles_y = (a.Y + kSlabTY - 1) / kSlabTY;
   const long long blocks = a.B * a.tiles_x * a.tiles_y;
   if (blocks == 0) return CIMX_OK;
