@@ -54,12 +54,56 @@ __device__ __forceinline__ float luma_u8(const uint8_t* p) {
   return y;
 }
 
+constexpr int kBR = 8;  // outputs per thread in the Gaussian passes
+constexpr int kBG = (kBT + 2 + kBR - 1) / kBR;  // 8-output groups over 66 rows or columns
+
+// acc[p] = the fused multiply-add chain over taps k = 0 .. K-1 of
+// x(p + k) * w[k], for kBR consecutive outputs p: the taps ascending from
+// +0 exactly as the one-output loop, with the inputs of a chunk of kBR taps
+// held in registers (each loaded once for the kBR outputs). `at(i)` may be
+// asked for up to 2 kBR - 1 inputs beyond the last one used.
+template <class At>
+__device__ __forceinline__ void chain_r(float (&acc)[kBR], const float* w, int K, At at) {
+  float win[2 * kBR];
+#pragma unroll
+  for (int j = 0; j < kBR; ++j) win[j] = at(j);
+  int k0 = 0;
+  for (; k0 + kBR <= K; k0 += kBR) {
+#pragma unroll
+    for (int j = 0; j < kBR; ++j) win[kBR + j] = at(k0 + kBR + j);
+#pragma unroll
+    for (int j = 0; j < kBR; ++j) {
+      const float t = w[k0 + j];
+#pragma unroll
+      for (int p = 0; p < kBR; ++p) acc[p] = fmaf(win[p + j], t, acc[p]);
+    }
+#pragma unroll
+    for (int j = 0; j < kBR; ++j) win[j] = win[kBR + j];
+  }
+  if (k0 < K) {
+#pragma unroll
+    for (int j = 0; j < kBR; ++j) win[kBR + j] = at(k0 + kBR + j);
+#pragma unroll
+    for (int j = 0; j < kBR; ++j) {
+      if (k0 + j < K) {
+        const float t = w[k0 + j];
+#pragma unroll
+        for (int p = 0; p < kBR; ++p) acc[p] = fmaf(win[p + j], t, acc[p]);
+      }
+    }
+  }
+}
+
 __global__ void __launch_bounds__(kBThreads, 2) k_batch_gray_gauss_sobel(const BatchArgs a) {
   extern __shared__ float smf[];
   __shared__ int s_tile;
+  __shared__ float s_w[kBMaxTaps];                 // this tile's taps
+  __shared__ int s_ci[kBT + 2], s_cj[kBT + 2];     // source row / column of each T row, S column
+  __shared__ int s_yc[kBG], s_xc[kBG];             // group of 8 with consecutive sources
   const int tid = threadIdx.x;
-  // strides sized for the batch's largest radius
-  const int gcs = kBT + 2 + 2 * a.max_r;  // row stride of the gray region and of T
+  // strides sized for the batch's largest radius; odd, so that lanes on
+  // consecutive rows read different banks
+  const int gcs = kBT + 3 + 2 * a.max_r;  // row stride of the gray region and of T
   float* G = smf;                          // (64 + 2 + 2r) rows x gcs
   float* T = smf + gcs * gcs;              // 66 rows x gcs
   // overlays of G once T exists: S (66 x 66), E0 (64 x 66), E1 (66 x 64)
@@ -98,6 +142,25 @@ __global__ void __launch_bounds__(kBThreads, 2) k_batch_gray_gauss_sobel(const B
     const float* w = a.taps + t.taps_offset;
     const int GR = kBT + 2 + 2 * r, GC = kBT + 2 + 2 * r;
 
+    // 0. the tile's taps, and the source row / column (in the gray region)
+    //    of every smoothed row / column the edge passes read: 'reflect'
+    //    around the tile, kept inside the region
+    for (int k = tid; k < K; k += kBThreads) s_w[k] = w[k];
+    for (int i = tid; i < kBT + 2; i += kBThreads) {
+      int ci = map_coord32(y0 - 1 + i, H, CIMX_MODE_REFLECT) - (y0 - 1 - r);
+      s_ci[i] = ci < r ? r : (ci > GR - 1 - r ? GR - 1 - r : ci);
+      int cj = map_coord32(x0 - 1 + i, W, CIMX_MODE_REFLECT) - (x0 - 1 - r);
+      s_cj[i] = cj < r ? r : (cj > GC - 1 - r ? GC - 1 - r : cj);
+    }
+    __syncthreads();
+    if (tid < 2 * kBG) {
+      const int q = tid % kBG, i0 = q * kBR;
+      const int* src = tid < kBG ? s_ci : s_cj;
+      int ok = i0 + kBR <= kBT + 2;
+      for (int p = 1; ok && p < kBR; ++p) ok = src[i0 + p] == src[i0] + p;
+      (tid < kBG ? s_yc : s_xc)[q] = ok;
+    }
+
     // 1. gray region: rows y0-1-r .., columns x0-1-r .., 'nearest' borders
     for (int idx = tid; idx < GR * GC; idx += kBThreads) {
       const int gr = idx / GC, c = idx - gr * GC;
@@ -107,28 +170,53 @@ __global__ void __launch_bounds__(kBThreads, 2) k_batch_gray_gauss_sobel(const B
     __syncthreads();
 
     // 2. gaussian along y: T row tr is the smoothed row refl(y0 - 1 + tr);
-    //    rows outside the tile only feed outputs that are not stored
-    for (int idx = tid; idx < (kBT + 2) * GC; idx += kBThreads) {
-      const int tr = idx / GC, c = idx - tr * GC;
-      int ci = map_coord32(y0 - 1 + tr, H, CIMX_MODE_REFLECT) - (y0 - 1 - r);
-      ci = ci < r ? r : (ci > GR - 1 - r ? GR - 1 - r : ci);
-      const float* col = G + (ci - r) * gcs + c;
-      float acc = 0.f;
-      for (int k = 0; k < K; ++k) acc = fmaf(col[k * gcs], w[k], acc);
-      T[tr * gcs + c] = acc;
+    //    rows outside the tile only feed outputs that are not stored. A
+    //    thread takes 8 consecutive T rows of one column; where their source
+    //    rows are not consecutive (tile borders) it runs them one by one.
+    for (int idx = tid; idx < kBG * GC; idx += kBThreads) {
+      const int q = idx / GC, c = idx - q * GC;
+      const int tr0 = q * kBR, nr = min(kBR, kBT + 2 - tr0);
+      if (s_yc[q]) {
+        float acc[kBR];
+#pragma unroll
+        for (int p = 0; p < kBR; ++p) acc[p] = 0.f;
+        const float* col = G + (s_ci[tr0] - r) * gcs + c;
+        chain_r(acc, s_w, K, [&](int i) { return col[i * gcs]; });
+#pragma unroll
+        for (int p = 0; p < kBR; ++p) T[(tr0 + p) * gcs + c] = acc[p];
+      } else {
+        for (int p = 0; p < nr; ++p) {
+          const float* col = G + (s_ci[tr0 + p] - r) * gcs + c;
+          float acc = 0.f;
+          for (int k = 0; k < K; ++k) acc = fmaf(col[k * gcs], s_w[k], acc);
+          T[(tr0 + p) * gcs + c] = acc;
+        }
+      }
     }
     __syncthreads();
 
     // 3. gaussian along x: S(sr, sc) is the smoothed value at
-    //    (refl(y0 - 1 + sr), refl(x0 - 1 + sc))
-    for (int idx = tid; idx < (kBT + 2) * (kBT + 2); idx += kBThreads) {
-      const int sr = idx / (kBT + 2), sc = idx - sr * (kBT + 2);
-      int cj = map_coord32(x0 - 1 + sc, W, CIMX_MODE_REFLECT) - (x0 - 1 - r);
-      cj = cj < r ? r : (cj > GC - 1 - r ? GC - 1 - r : cj);
-      const float* row = T + sr * gcs + (cj - r);
-      float acc = 0.f;
-      for (int k = 0; k < K; ++k) acc = fmaf(row[k], w[k], acc);
-      S[idx] = acc;
+    //    (refl(y0 - 1 + sr), refl(x0 - 1 + sc)); a thread takes 8
+    //    consecutive columns of one row (lanes on consecutive rows)
+    for (int idx = tid; idx < kBG * (kBT + 2); idx += kBThreads) {
+      const int q = idx / (kBT + 2), sr = idx - q * (kBT + 2);
+      const int sc0 = q * kBR, nc = min(kBR, kBT + 2 - sc0);
+      if (s_xc[q]) {
+        float acc[kBR];
+#pragma unroll
+        for (int p = 0; p < kBR; ++p) acc[p] = 0.f;
+        const float* row = T + sr * gcs + (s_cj[sc0] - r);
+        chain_r(acc, s_w, K, [&](int i) { return row[i]; });
+#pragma unroll
+        for (int p = 0; p < kBR; ++p) S[sr * (kBT + 2) + sc0 + p] = acc[p];
+      } else {
+        for (int p = 0; p < nc; ++p) {
+          const float* row = T + sr * gcs + (s_cj[sc0 + p] - r);
+          float acc = 0.f;
+          for (int k = 0; k < K; ++k) acc = fmaf(row[k], s_w[k], acc);
+          S[sr * (kBT + 2) + sc0 + p] = acc;
+        }
+      }
     }
     __syncthreads();
 
@@ -200,12 +288,15 @@ extern "C" int cimx_batch_gray_gauss_sobel(const CimxBatchTile* tiles, int ntile
   }
   // gray region + T, or S + E0 + E1 (which overlay the gray region and
   // spill into T for small radii), whichever is larger
-  const int gcs = kBT + 2 + 2 * a.max_r;
-  const size_t region = static_cast<size_t>(gcs) * gcs + static_cast<size_t>(kBT + 2) * gcs;
+  const int gcs = kBT + 3 + 2 * a.max_r;
+  // the register-blocked chains read up to 2 * 8 - 1 inputs past the last
+  // one they use: slack after T for its last row
+  const size_t region = static_cast<size_t>(gcs) * gcs + static_cast<size_t>(kBT + 2) * gcs + 64;
   const size_t overlay = static_cast<size_t>(kBT + 2) * (kBT + 2) + 2 * kBT * (kBT + 2);
   const size_t smem = sizeof(float) * std::max(region, overlay);
-  // the kernel also holds a few bytes of static shared memory
-  constexpr int kDynLimit = 226 * 1024;
+  // the kernel also holds about 1.2 KB of static shared memory (taps and
+  // the row / column tables); the sum stays under the 227 KB per CTA
+  constexpr int kDynLimit = 225 * 1024;
   if (smem > static_cast<size_t>(kDynLimit)) return fail(CIMX_E_INVALID, "batch: taps too long");
   static std::once_flag once;
   static cudaError_t attr_err = cudaSuccess;
