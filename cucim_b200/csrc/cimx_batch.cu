@@ -5,7 +5,8 @@
 // skimage.filters.sobel (color/colorconv.py:1038-1095,
 // _shared/filters.py:21-166, filters/edges.py:148-306), computed with exactly
 // the arithmetic of the per-tile path of this library:
-//   gray  = (float)(0.2125 r + 0.7154 g + 0.0721 b) in float64, r = (float)u8 * (float)(1/255);
+//   gray  = (float)(0.0721 b + (0.2125 r + 0.7154 g)) in float64 fused multiply-adds,
+//           r = (float)u8 * (float)(1/255) (a 256-entry table of the float64 values);
 //   T     = gaussian along y of gray (float32 FMA chain, taps ascending, from +0),
 //   S     = gaussian along x of T, both with 'nearest' borders;
 //   d0    = smooth along x of (edge along y of S), d1 = smooth along y of (edge along x of S),
@@ -45,15 +46,20 @@ struct BatchArgs {
 
 __device__ __forceinline__ int nearest_idx(int i, int n) { return i < 0 ? 0 : (i >= n ? n - 1 : i); }
 
-__device__ __forceinline__ float luma_u8(const uint8_t* p) {
-  const float s = static_cast<float>(1.0 / 255.0);
-  const float r = __fmul_rn(static_cast<float>(p[0]), s);
-  const float g = __fmul_rn(static_cast<float>(p[1]), s);
-  const float b = __fmul_rn(static_cast<float>(p[2]), s);
-  float y = 0.2125 * r + 0.7154 * g + 0.0721 * b;
-  return y;
+// The float64 value of one channel: (double)((float)u * (float)(1/255)).
+__device__ __forceinline__ double channel_f64(int u) {
+  return static_cast<double>(__fmul_rn(static_cast<float>(u), static_cast<float>(1.0 / 255.0)));
 }
 
+// gray = (float)(0.2125 r + 0.7154 g + 0.0721 b) with the float64
+// operations in the order the per-tile rgb2gray kernel contracts them:
+// 0.0721 b + (0.2125 r + 0.7154 g), each sum a fused multiply-add.
+__device__ __forceinline__ float luma_f64(double r, double g, double b) {
+  return __double2float_rn(__fma_rn(0.0721, b, __fma_rn(0.2125, r, __dmul_rn(0.7154, g))));
+}
+
+constexpr int kSS = kBT + 3;  // row stride of S: odd, for the column-wise writes of the x pass
+constexpr int kGB = 4;  // 4-pixel groups whose words a thread loads at once (gray step)
 constexpr int kBR = 8;  // outputs per thread in the Gaussian passes
 constexpr int kBG = (kBT + 2 + kBR - 1) / kBR;  // 8-output groups over 66 rows or columns
 
@@ -96,33 +102,47 @@ __device__ __forceinline__ void chain_r(float (&acc)[kBR], const float* w, int K
 
 __global__ void __launch_bounds__(kBThreads, 2) k_batch_gray_gauss_sobel(const BatchArgs a) {
   extern __shared__ float smf[];
-  __shared__ int s_tile;
+  __shared__ CimxBatchTile s_t;                    // this block's tile
   __shared__ float s_w[kBMaxTaps];                 // this tile's taps
   __shared__ int s_ci[kBT + 2], s_cj[kBT + 2];     // source row / column of each T row, S column
   __shared__ int s_yc[kBG], s_xc[kBG];             // group of 8 with consecutive sources
+  __shared__ double s_ch[256];                     // channel_f64 of every byte value
   const int tid = threadIdx.x;
+  for (int u = tid; u < 256; u += kBThreads) s_ch[u] = channel_f64(u);
   // strides sized for the batch's largest radius; odd, so that lanes on
   // consecutive rows read different banks
   const int gcs = kBT + 3 + 2 * a.max_r;  // row stride of the gray region and of T
   float* G = smf;                          // (64 + 2 + 2r) rows x gcs
   float* T = smf + gcs * gcs;              // 66 rows x gcs
-  // overlays of G once T exists: S (66 x 66), E0 (64 x 66), E1 (66 x 64)
+  // overlays of G once T exists: S (66 x 66, row stride kSS), E0 (64 x 66),
+  // E1 (66 x 64)
   float* S = smf;
-  float* E0 = S + (kBT + 2) * (kBT + 2);
+  float* E0 = S + (kBT + 2) * kSS;
   float* E1 = E0 + kBT * (kBT + 2);
 
   for (long long g = blockIdx.x; g < a.nblocks; g += gridDim.x) {
-    if (tid == 0) {
-      int lo = 0, hi = a.ntiles - 1;  // last tile whose first block <= g
-      while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (a.tiles[mid].first_block <= g) lo = mid;
-        else hi = mid - 1;
+    if (tid < 32) {
+      // the last tile whose first block <= g, found by the first warp: each
+      // round probes 32 evenly spaced tiles of (lo, hi] and keeps the span
+      // between the last probe <= g and the next one (three rounds for
+      // 4096 tiles)
+      int lo = 0, hi = a.ntiles - 1;
+      while (hi > lo) {
+        const int step = (hi - lo + 31) / 32;
+        const int cand = lo + 1 + tid * step;
+        const bool le = cand <= hi && a.tiles[cand].first_block <= g;
+        const int nle = __popc(__ballot_sync(0xffffffffu, le));
+        if (nle == 0) {
+          hi = lo;
+        } else {
+          lo += 1 + (nle - 1) * step;
+          hi = min(hi, lo + step - 1);
+        }
       }
-      s_tile = lo;
+      if (tid == 0) s_t = a.tiles[lo];
     }
     __syncthreads();
-    const CimxBatchTile t = a.tiles[s_tile];
+    const CimxBatchTile& t = s_t;
     const int H = t.height, W = t.width;
     // row pitches: a tile may be a region of a larger slide (0 = packed)
     const long long in_pitch = t.rgb_pitch > 0 ? t.rgb_pitch : 3LL * W;
@@ -161,11 +181,63 @@ __global__ void __launch_bounds__(kBThreads, 2) k_batch_gray_gauss_sobel(const B
       (tid < kBG ? s_yc : s_xc)[q] = ok;
     }
 
-    // 1. gray region: rows y0-1-r .., columns x0-1-r .., 'nearest' borders
-    for (int idx = tid; idx < GR * GC; idx += kBThreads) {
-      const int gr = idx / GC, c = idx - gr * GC;
-      const int gy = nearest_idx(y0 - 1 - r + gr, H), gx = nearest_idx(x0 - 1 - r + c, W);
-      G[gr * gcs + c] = luma_u8(t.rgb + static_cast<long long>(gy) * in_pitch + gx * 3LL);
+    // 1. gray region: rows y0-1-r .., columns x0-1-r .., 'nearest' borders.
+    //    A thread takes groups of 4 consecutive pixels of a row: where they
+    //    lie inside the row, their 12 bytes come from three or four aligned
+    //    32-bit words (each word holds at least one of the 12 bytes, so it
+    //    lies in the tile's allocation); at the tile's borders pixel by
+    //    pixel. The words of kGB groups are loaded before any is used.
+    {
+      const int GC4 = (GC + 3) >> 2, ng = GR * GC4;
+      const int xb = x0 - 1 - r;  // source column of region column 0
+      for (int i0 = tid; i0 < ng; i0 += kGB * kBThreads) {
+        uint32_t wv[kGB][4];
+        unsigned shv[kGB];
+        bool fast[kGB];
+#pragma unroll
+        for (int u = 0; u < kGB; ++u) {
+          const int idx = i0 + u * kBThreads;
+          const int gr = idx / GC4, c0 = (idx - gr * GC4) * 4;
+          const int xs = xb + c0;
+          fast[u] = idx < ng && xs >= 0 && xs + 3 < W && c0 + 3 < GC;
+          shv[u] = 0;
+          wv[u][0] = wv[u][1] = wv[u][2] = wv[u][3] = 0u;
+          if (fast[u]) {
+            const uint8_t* px = t.rgb + static_cast<long long>(nearest_idx(y0 - 1 - r + gr, H)) * in_pitch + 3LL * xs;
+            const uintptr_t pa = reinterpret_cast<uintptr_t>(px);
+            const uint32_t* wp = reinterpret_cast<const uint32_t*>(pa & ~static_cast<uintptr_t>(3));
+            shv[u] = static_cast<unsigned>(pa & 3) * 8u;
+            wv[u][0] = __ldg(wp);
+            wv[u][1] = __ldg(wp + 1);
+            wv[u][2] = __ldg(wp + 2);
+            if (shv[u]) wv[u][3] = __ldg(wp + 3);
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < kGB; ++u) {
+          const int idx = i0 + u * kBThreads;
+          if (idx >= ng) break;
+          const int gr = idx / GC4, c0 = (idx - gr * GC4) * 4;
+          float* dst = G + gr * gcs + c0;
+          if (fast[u]) {
+            const unsigned sh = shv[u];
+            const uint32_t v0 = __funnelshift_r(wv[u][0], wv[u][1], sh);
+            const uint32_t v1 = __funnelshift_r(wv[u][1], wv[u][2], sh);
+            const uint32_t v2 = __funnelshift_r(wv[u][2], wv[u][3], sh);
+            dst[0] = luma_f64(s_ch[v0 & 255u], s_ch[(v0 >> 8) & 255u], s_ch[(v0 >> 16) & 255u]);
+            dst[1] = luma_f64(s_ch[v0 >> 24], s_ch[v1 & 255u], s_ch[(v1 >> 8) & 255u]);
+            dst[2] = luma_f64(s_ch[(v1 >> 16) & 255u], s_ch[v1 >> 24], s_ch[v2 & 255u]);
+            dst[3] = luma_f64(s_ch[(v2 >> 8) & 255u], s_ch[(v2 >> 16) & 255u], s_ch[v2 >> 24]);
+          } else {
+            const uint8_t* row = t.rgb + static_cast<long long>(nearest_idx(y0 - 1 - r + gr, H)) * in_pitch;
+            const int xs = xb + c0;
+            for (int p = 0; p < 4 && c0 + p < GC; ++p) {
+              const uint8_t* px = row + 3LL * nearest_idx(xs + p, W);
+              dst[p] = luma_f64(s_ch[px[0]], s_ch[px[1]], s_ch[px[2]]);
+            }
+          }
+        }
+      }
     }
     __syncthreads();
 
@@ -208,13 +280,13 @@ __global__ void __launch_bounds__(kBThreads, 2) k_batch_gray_gauss_sobel(const B
         const float* row = T + sr * gcs + (s_cj[sc0] - r);
         chain_r(acc, s_w, K, [&](int i) { return row[i]; });
 #pragma unroll
-        for (int p = 0; p < kBR; ++p) S[sr * (kBT + 2) + sc0 + p] = acc[p];
+        for (int p = 0; p < kBR; ++p) S[sr * kSS + sc0 + p] = acc[p];
       } else {
         for (int p = 0; p < nc; ++p) {
           const float* row = T + sr * gcs + (s_cj[sc0 + p] - r);
           float acc = 0.f;
           for (int k = 0; k < K; ++k) acc = fmaf(row[k], s_w[k], acc);
-          S[sr * (kBT + 2) + sc0 + p] = acc;
+          S[sr * kSS + sc0 + p] = acc;
         }
       }
     }
@@ -224,14 +296,14 @@ __global__ void __launch_bounds__(kBThreads, 2) k_batch_gray_gauss_sobel(const B
     for (int idx = tid; idx < kBT * (kBT + 2); idx += kBThreads) {
       const int y = idx / (kBT + 2), sc = idx - y * (kBT + 2);
       float acc = 0.f;
-      acc = fmaf(S[y * (kBT + 2) + sc], a.edge[0], acc);
-      acc = fmaf(S[(y + 1) * (kBT + 2) + sc], a.edge[1], acc);
-      acc = fmaf(S[(y + 2) * (kBT + 2) + sc], a.edge[2], acc);
+      acc = fmaf(S[y * kSS + sc], a.edge[0], acc);
+      acc = fmaf(S[(y + 1) * kSS + sc], a.edge[1], acc);
+      acc = fmaf(S[(y + 2) * kSS + sc], a.edge[2], acc);
       E0[idx] = acc;
     }
     for (int idx = tid; idx < (kBT + 2) * kBT; idx += kBThreads) {
       const int sr = idx / kBT, x = idx - sr * kBT;
-      const float* row = S + sr * (kBT + 2) + x;
+      const float* row = S + sr * kSS + x;
       float acc = 0.f;
       acc = fmaf(row[0], a.edge[0], acc);
       acc = fmaf(row[1], a.edge[1], acc);
@@ -292,11 +364,12 @@ extern "C" int cimx_batch_gray_gauss_sobel(const CimxBatchTile* tiles, int ntile
   // the register-blocked chains read up to 2 * 8 - 1 inputs past the last
   // one they use: slack after T for its last row
   const size_t region = static_cast<size_t>(gcs) * gcs + static_cast<size_t>(kBT + 2) * gcs + 64;
-  const size_t overlay = static_cast<size_t>(kBT + 2) * (kBT + 2) + 2 * kBT * (kBT + 2);
+  const size_t overlay = static_cast<size_t>(kBT + 2) * kSS + 2 * kBT * (kBT + 2);
   const size_t smem = sizeof(float) * std::max(region, overlay);
-  // the kernel also holds about 1.2 KB of static shared memory (taps and
-  // the row / column tables); the sum stays under the 227 KB per CTA
-  constexpr int kDynLimit = 225 * 1024;
+  // the kernel also holds about 3.2 KB of static shared memory (taps, the
+  // row / column tables, the channel table); the sum stays under the 227 KB
+  // per CTA
+  constexpr int kDynLimit = 223 * 1024;
   if (smem > static_cast<size_t>(kDynLimit)) return fail(CIMX_E_INVALID, "batch: taps too long");
   static std::once_flag once;
   static cudaError_t attr_err = cudaSuccess;
