@@ -23,6 +23,8 @@ _NP_TO_TORCH = {
     np.dtype(np.float16): torch.float16,
     np.dtype(np.float32): torch.float32,
     np.dtype(np.float64): torch.float64,
+    np.dtype(np.complex64): torch.complex64,
+    np.dtype(np.complex128): torch.complex128,
     np.dtype(np.bool_): torch.bool,
 }
 _TORCH_TO_NP = {v: k for k, v in _NP_TO_TORCH.items()}

@@ -36,6 +36,7 @@ F_W64 = 1 << 0
 F_CONVOLVE = 1 << 1
 F_CVAL_AS_INPUT = 1 << 2
 F_SKIP_ZERO_TAPS = 1 << 3
+F_COMPLEX_TAPS = 1 << 4
 L_NO_FUSION = 1 << 0
 L_TENSOR_BF16X3 = 1 << 1
 L_TENSOR_TF32X3 = 1 << 2
@@ -240,6 +241,11 @@ def check(rc, what):
 
 
 def taps_pointer(taps):
-    """A float64 C-contiguous copy of `taps` and a pointer into it."""
-    t = np.ascontiguousarray(np.asarray(taps, dtype=np.float64))
+    """A float64 C-contiguous copy of `taps` and a pointer into it; complex
+    taps become (re, im) pairs (CIMX_F_COMPLEX_TAPS)."""
+    taps = np.asarray(taps)
+    if taps.dtype.kind == "c":
+        t = np.ascontiguousarray(taps, dtype=np.complex128).view(np.float64)
+    else:
+        t = np.ascontiguousarray(taps, dtype=np.float64)
     return t, t.ctypes.data_as(_P(ctypes.c_double))

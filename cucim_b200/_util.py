@@ -44,11 +44,13 @@ def supported_float_type(input_dtype, allow_complex=False):
 
 
 def weights_dtype(input_dtype, w_dtype):
-    """UTIL:35-46 with use_cucim_casting=True (real dtypes)."""
+    """UTIL:35-46 with use_cucim_casting=True: complex64 / complex128 when the
+    input or the weights are complex."""
     w_dtype = np.dtype(w_dtype)
     in_dtype = np.dtype(input_dtype)
     if w_dtype.kind == "c" or in_dtype.kind == "c":
-        raise NotImplementedError("complex arrays are not supported")
+        real = in_dtype if in_dtype.kind != "c" else np.empty(0, in_dtype).real.dtype
+        return np.promote_types(real, np.complex64)
     if w_dtype.kind in "iub":
         return supported_float_type(w_dtype)
     return np.promote_types(in_dtype, np.float32)
@@ -183,8 +185,10 @@ def _pass_flags(in_dtype, ndim, axis, K, origin, mode, cval, w_dtype, convolve, 
     anchor = K // 2 + o
     alg = choose_algorithm(ndim, axis, K, anchor, mode, cval, in_dtype, algorithm)
     flags = 0
-    if wdt == np.float64:
+    if wdt in (np.float64, np.complex128):
         flags |= _lib.F_W64
+    if np.dtype(w_dtype).kind == "c":
+        flags |= _lib.F_COMPLEX_TAPS
     if convolve:
         flags |= _lib.F_CONVOLVE
     if alg == "shared_memory":

@@ -90,7 +90,7 @@ void scratch_free(void* p, size_t nbytes, cudaStream_t s) {
 
 namespace {
 
-bool supported_dtype(int dt) { return dtype_size(dt) > 0; }
+bool supported_dtype(int dt) { return element_size(dt) > 0; }
 
 int64_t numel(const CimxArray* a) {
   int64_t n = 1;
@@ -100,7 +100,7 @@ int64_t numel(const CimxArray* a) {
 
 bool c_contiguous(const CimxArray* a) {
   if (numel(a) == 0) return true;
-  int64_t expect = dtype_size(a->dtype);
+  int64_t expect = element_size(a->dtype);
   for (int d = a->ndim - 1; d >= 0; --d) {
     if (a->shape[d] != 1 && a->strides[d] != expect) return false;
     expect *= a->shape[d];
@@ -132,8 +132,8 @@ int check_same_shape(const CimxArray* a, const CimxArray* b) {
 bool overlaps(const CimxArray* a, const CimxArray* b) {
   const char* a0 = static_cast<const char*>(a->data);
   const char* b0 = static_cast<const char*>(b->data);
-  const char* a1 = a0 + numel(a) * dtype_size(a->dtype);
-  const char* b1 = b0 + numel(b) * dtype_size(b->dtype);
+  const char* a1 = a0 + numel(a) * element_size(a->dtype);
+  const char* b1 = b0 + numel(b) * element_size(b->dtype);
   return numel(a) > 0 && numel(b) > 0 && a0 < b1 && b0 < a1;
 }
 
@@ -159,9 +159,18 @@ int make_pass(const CimxArray* shape_of, const CimxPass& p, std::vector<double>&
   const int K = p.ntaps;
   int origin = p.origin;
   if (K / 2 + origin < 0 || K / 2 + origin >= K) return fail(CIMX_E_INVALID, "invalid origin");
-  taps_store.assign(p.taps, p.taps + K);
+  const bool ctaps = (p.flags & CIMX_F_COMPLEX_TAPS) != 0;
+  taps_store.assign(p.taps, p.taps + (ctaps ? 2 * K : K));
   if (p.flags & CIMX_F_CONVOLVE) {
-    std::reverse(taps_store.begin(), taps_store.end());
+    if (ctaps) {
+      // reverse the (re, im) pairs
+      for (int i = 0, j = K - 1; i < j; ++i, --j) {
+        std::swap(taps_store[2 * i], taps_store[2 * j]);
+        std::swap(taps_store[2 * i + 1], taps_store[2 * j + 1]);
+      }
+    } else {
+      std::reverse(taps_store.begin(), taps_store.end());
+    }
     origin = -origin;
     if (K % 2 == 0) origin -= 1;
   }
@@ -178,6 +187,7 @@ int make_pass(const CimxArray* shape_of, const CimxPass& p, std::vector<double>&
   d.w64 = (p.flags & CIMX_F_W64) != 0;
   d.cval_as_input = (p.flags & CIMX_F_CVAL_AS_INPUT) != 0;
   d.skip_zero = (p.flags & CIMX_F_SKIP_ZERO_TAPS) != 0;
+  d.ctaps = ctaps;
   d.taps = taps_store.data();
   return CIMX_OK;
 }
@@ -222,6 +232,8 @@ int cimx_correlate1d(const CimxArray* in, const CimxArray* out, const double* ta
   d.out = out->data;
   d.tin = in->dtype;
   d.tout = out->dtype;
+  if (is_complex_dt(in->dtype) || is_complex_dt(out->dtype) || d.ctaps)
+    return complex_separable(in, out, &d, 1, static_cast<cudaStream_t>(stream));
   return launch_generic_pass(d, static_cast<cudaStream_t>(stream));
 }
 
@@ -235,14 +247,23 @@ int cimx_separable(const CimxArray* in, const CimxArray* out, const CimxPass* pa
   if (npasses < 0 || (npasses > 0 && !passes)) return fail(CIMX_E_INVALID, "bad pass list");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const int64_t n = numel(in);
-  if (npasses == 0) return launch_copy_cast(in->data, in->dtype, out->data, out->dtype, n, st);
+  const bool cplx = is_complex_dt(in->dtype) || is_complex_dt(out->dtype);
+  if (npasses == 0) {
+    if (cplx) return complex_separable(in, out, nullptr, 0, st);
+    return launch_copy_cast(in->data, in->dtype, out->data, out->dtype, n, st);
+  }
   if (in->ndim == 0) return fail(CIMX_E_INVALID, "separable filtering needs ndim >= 1");
 
   std::vector<std::vector<double>> taps(npasses);
   std::vector<PassDesc> ds(npasses);
+  bool ctaps = false;
   for (int i = 0; i < npasses; ++i) {
     if ((rc = make_pass(in, passes[i], taps[i], ds[i]))) return rc;
+    ctaps = ctaps || ds[i].ctaps;
   }
+  // complex arrays or taps: cuCIM's complex<float> / complex<double> kernels,
+  // one launch per pass
+  if (cplx || ctaps) return complex_separable(in, out, ds.data(), npasses, st);
   if (n == 0) return CIMX_OK;
 
   // the autotuner's schedule for this signature (or the caller's flags)

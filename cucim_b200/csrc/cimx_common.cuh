@@ -23,7 +23,7 @@ namespace cimx {
 enum : int {
   DT_U8 = 'B', DT_I8 = 'b', DT_U16 = 'H', DT_I16 = 'h', DT_U32 = 'I', DT_I32 = 'i',
   DT_U64 = 'L', DT_U64Q = 'Q', DT_I64 = 'l', DT_I64Q = 'q', DT_F16 = 'e', DT_F32 = 'f',
-  DT_F64 = 'd',
+  DT_F64 = 'd', DT_C64 = 'F', DT_C128 = 'D',
 };
 
 __host__ __device__ inline int dtype_size(int dt) {
@@ -34,6 +34,14 @@ __host__ __device__ inline int dtype_size(int dt) {
     case DT_U64: case DT_U64Q: case DT_I64: case DT_I64Q: case DT_F64: return 8;
     default: return 0;
   }
+}
+
+// complex64 / complex128: taken only by the entries that filter complex
+// arrays (cimx_correlate1d, cimx_separable); dtype_size() leaves them out so
+// every other entry rejects them as unsupported
+__host__ __device__ inline bool is_complex_dt(int dt) { return dt == DT_C64 || dt == DT_C128; }
+__host__ __device__ inline int element_size(int dt) {
+  return dt == DT_C64 ? 8 : dt == DT_C128 ? 16 : dtype_size(dt);
 }
 
 // ---------------------------------------------------------------- casts

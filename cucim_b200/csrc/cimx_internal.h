@@ -34,6 +34,7 @@ struct PassDesc {
   bool cval_as_input;
   bool skip_zero;  // skip zero taps (only matters for non-finite inputs)
   bool no_alloc;   // the pass must not take scratch memory (cimx_separable_noalloc)
+  bool ctaps;      // taps are K (re, im) pairs (CIMX_F_COMPLEX_TAPS)
   const double* taps;  // host taps, already flipped for convolution, not yet rounded
 };
 
@@ -65,6 +66,13 @@ int tuned_flags(const std::string& key, int lib_flags, cudaStream_t st,
 
 // generic single pass (cimx_pass.cu)
 int launch_generic_pass(const PassDesc& d, cudaStream_t stream);
+
+// Passes over complex arrays or with complex taps (cimx_complex.cu): cuCIM's
+// complex<float> / complex<double> arithmetic, one launch per pass through
+// one scratch array of the output dtype. ds[i].in/out/tin/tout are set here.
+// npasses == 0 copies `in` into `out` with a complex conversion.
+int complex_separable(const CimxArray* in, const CimxArray* out, PassDesc* ds, int npasses,
+                      cudaStream_t st);
 
 // elementwise helpers (cimx_elementwise.cu)
 int launch_square_accumulate(void* acc, const void* term, int dt, int64_t n, bool first,

@@ -38,7 +38,9 @@ class _PassList:
         t, ptr = _lib.taps_pointer(taps)
         self.keep.append(t)
         p = _lib.CimxPass()
-        p.axis, p.ntaps, p.origin = axis, t.size, origin
+        # complex taps are (re, im) pairs in t
+        ntaps = t.size // 2 if flags & _lib.F_COMPLEX_TAPS else t.size
+        p.axis, p.ntaps, p.origin = axis, ntaps, origin
         p.mode, p.cval, p.flags, p.reserved = _lib.MODE_CODES[mode], float(cval), flags, 0
         p.taps = ptr
         self.items.append(p)
@@ -70,8 +72,6 @@ def _build_passes(in_dtype, out_dtype, ndim, specs, cval, algorithm):
         w = np.asarray(w)
         if w.ndim != 1 or w.size < 1:
             raise RuntimeError("incorrect filter size")
-        if w.dtype.kind == "c":
-            raise NotImplementedError("complex weights are not supported")
         K = w.size
         axis = _util.normalize_axis(axis, ndim)
         origin = _util.check_origin(origin, K)
@@ -173,14 +173,38 @@ def tensor_cores_everywhere():
         _EXTRA_LIB_FLAGS = old
 
 
-def _run(input, specs, output, cval, algorithm=None, cache_key=None):
+def _complex_output(output, in_dt):
+    """_get_output (UTIL:49-71) when the output is complex: the default is
+    the input's dtype promoted to complex64; a dtype-like real output is
+    promoted with a warning, a dtype name or an array must be complex."""
+    if output is None:
+        return None, np.promote_types(in_dt, np.complex64)
+    if isinstance(output, str):
+        if np.dtype(output).kind != "c":
+            raise RuntimeError("output must have complex dtype")
+        return output, None
+    if _arrays.is_dtype_like(output):
+        dt = _arrays.np_dtype(output) if isinstance(output, torch.dtype) else np.dtype(output)
+        if dt.kind != "c":
+            warnings.warn("promoting specified output dtype to complex")
+            return np.promote_types(dt, np.complex64), None
+        return output, None
+    if _arrays.np_dtype(_arrays.as_tensor(output)).kind != "c":
+        raise RuntimeError("output must have complex dtype")
+    return output, None
+
+
+def _run(input, specs, output, cval, algorithm=None, cache_key=None, complex_weights=False):
     """Apply the pass list to `input` into `output` (FLT:363-396 semantics).
-    `cache_key`: a hashable description of `specs` (None: not cached)."""
+    `cache_key`: a hashable description of `specs` (None: not cached).
+    Complex input or weights give a complex output (CORE:195-203)."""
     x = _arrays.as_tensor(input)
-    if x.dtype.is_complex:
-        raise NotImplementedError("complex arrays are not supported")
     xc = x.contiguous()
-    slot = _arrays.output_slot(output, input, xc)
+    if x.dtype.is_complex or complex_weights:
+        output, default_dt = _complex_output(output, _arrays.np_dtype(xc))
+        slot = _arrays.output_slot(output, input, xc, dtype=default_dt)
+    else:
+        slot = _arrays.output_slot(output, input, xc)
     out_dt = slot.dtype
     lib_flags = _EXTRA_LIB_FLAGS
     if algorithm in _TENSOR_FLAGS:
@@ -212,6 +236,9 @@ def _correlate_or_convolve1d(input, weights, axis, output, mode, cval, origin,
     x = _arrays.as_tensor(input)
     axis = _util.normalize_axis(axis, x.dim())
     w = _weights_to_host(weights)
+    if not convolution and w.dtype.kind == "c":
+        # numpy.correlate conjugates the weights rather than the input
+        w = w.conj()
     if algorithm not in (None, "shared_memory", "elementwise", TENSOR, TENSOR_BF16X3):
         raise ValueError("algorithm must be 'shared_memory', 'elementwise' or None")
     if algorithm == "shared_memory" and mode == "constant" and (
@@ -221,7 +248,8 @@ def _correlate_or_convolve1d(input, weights, axis, output, mode, cval, origin,
             f"{cval=} and input.dtype={_arrays.np_dtype(x)} is unsupported for algorithm "
             "'shared_memory', falling back to elementwise"
         )
-    return _run(input, [(axis, w, mode, origin, convolution)], output, cval, algorithm)
+    return _run(input, [(axis, w, mode, origin, convolution)], output, cval, algorithm,
+                complex_weights=w.dtype.kind == "c")
 
 
 def _weights_to_host(weights):

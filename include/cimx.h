@@ -37,7 +37,10 @@ extern "C" {
 #define CIMX_MAX_NDIM 8
 
 /* Element types: the numpy dtype.char of the array ('B','b','H','h','I','i',
- * 'L'/'Q','l'/'q','e','f','d'). */
+ * 'L'/'Q','l'/'q','e','f','d'). cimx_correlate1d and cimx_separable also take
+ * complex64 'F' and complex128 'D' (cuCIM's complex<float> / complex<double>
+ * kernels, _vendored/_ndimage_util.py:35-37: W is complex whenever the input or
+ * the weights are; the output must then be complex). */
 typedef struct CimxArray {
   void* data;                       /* device pointer */
   int32_t dtype;                    /* numpy dtype.char, e.g. 'f' */
@@ -65,6 +68,11 @@ enum {
                                    (_vendored/_ndimage_filters_core.py:334-348) */
   CIMX_F_SKIP_ZERO_TAPS = 1 << 3,/* zero taps are skipped, as the elementwise kernel does
                                    (_vendored/_ndimage_filters_core.py:307-309) */
+  CIMX_F_COMPLEX_TAPS = 1 << 4, /* `taps` holds K (re, im) pairs: complex weights. W is then
+                                   complex<float> (complex<double> with CIMX_F_W64); the
+                                   output must be complex64 or complex128. The taps are used
+                                   as given: correlate1d's conjugation of complex weights
+                                   (_vendored/_ndimage_filters.py:242-244) is the caller's */
 };
 
 /* Library-level flags for multi-pass calls. */

@@ -93,6 +93,10 @@ def supported_float_type(dt):
 def weights_dtype(input_dtype, w_dtype):
     """UTIL:35-46 with use_cucim_casting=True."""
     w_dtype = np.dtype(w_dtype)
+    in_dtype = np.dtype(input_dtype)
+    if w_dtype.kind == "c" or in_dtype.kind == "c":
+        real = np.empty(0, in_dtype).real.dtype
+        return np.promote_types(real, np.complex64)
     if w_dtype.kind in "iub":
         return supported_float_type(w_dtype)
     return np.promote_types(np.dtype(input_dtype), np.float32)
@@ -260,15 +264,25 @@ def pass_params(in_dtype, ndim, axis, weights, mode, cval, origin, convolve, alg
     return taps, anchor, MODES[mode], cval_w, int(w64), int(skip_zero), path
 
 
-def get_output(output, input, shape=None):
-    """UTIL:49-71 (real dtypes only)."""
+def get_output(output, input, shape=None, complex_output=False):
+    """UTIL:49-71."""
     shape = input.shape if shape is None else shape
     if output is None:
-        return np.empty(shape, dtype=input.dtype)
-    if isinstance(output, (type, np.dtype, str)):
+        dt = np.promote_types(input.dtype, np.complex64) if complex_output else input.dtype
+        return np.empty(shape, dtype=dt)
+    if isinstance(output, str):
+        if complex_output and np.dtype(output).kind != "c":
+            raise RuntimeError("output must have complex dtype")
         return np.empty(shape, dtype=np.dtype(output))
+    if isinstance(output, (type, np.dtype)):
+        dt = np.dtype(output)
+        if complex_output and dt.kind != "c":
+            dt = np.promote_types(dt, np.complex64)
+        return np.empty(shape, dtype=dt)
     if output.shape != shape:
         raise RuntimeError("output shape not correct")
+    if complex_output and output.dtype.kind != "c":
+        raise RuntimeError("output must have complex dtype")
     return output
 
 
@@ -290,10 +304,112 @@ def _run_pass(x, out, axis, taps, anchor, mode_code, cval_w, w64, skip_zero):
     return out
 
 
+def _map_coords(ix, n, mode):
+    """UTIL:186-308 on an index array: the coordinate each index reads, -1
+    outside the array in constant mode."""
+    ix = np.asarray(ix, dtype=np.int64)
+    inside = (ix >= 0) & (ix < n)
+    if mode == "constant":
+        return np.where(inside, ix, -1)
+    if mode == "nearest":
+        return np.clip(ix, 0, n - 1)
+    if mode == "grid-wrap":
+        return np.mod(ix, n)
+    if mode in ("reflect", "grid-mirror"):
+        m = np.where(ix < 0, -1 - ix, ix) % (2 * n)
+        return np.where(inside, ix, np.minimum(m, 2 * n - 1 - m))
+    if mode == "mirror":
+        if n == 1:
+            return np.zeros_like(ix)
+        m = np.abs(ix)
+        m = 1 + (m - 1) % (2 * n - 2)
+        return np.where(inside, ix, np.minimum(m, 2 * n - 2 - m))
+    raise RuntimeError(f"boundary mode not supported (actual: {mode})")
+
+
+def _complex_correlate1d(input, weights, axis, out, mode, cval, origin, algorithm, convolve):
+    """cuCIM's correlate kernels instantiated with W = complex<float> /
+    complex<double> (FLT:224-244, CORE:195-203, SEP:720-760). Per output:
+    sum = (W)0, then for each tap (skipped by the elementwise kernel when it
+    is 0 + 0i) sum = sum + value * w with the complex product
+    (x.r w.r - x.i w.i, x.i w.r + x.r w.i) contracted into
+    p.r = fma(x.r, w.r, -(x.i w.i)), p.i = fma(x.i, w.r, x.r w.i) and each
+    part added with one rounding; out = (D)sum part by part. value: the
+    input's parts; a real input x is (x, +0), except in the elementwise
+    kernel outside constant mode, whose cast<W>() rule gives a negative or
+    NaN float x the imaginary part -0; the fill value is cast<W>(cval)
+    (elementwise) or (W)(T)cval (shared memory)."""
+    x = np.asarray(input)
+    weights = np.asarray(weights)
+    K = weights.size
+    origin = check_origin(origin, K)
+    if mode == "wrap":
+        mode = "grid-wrap"
+    check_mode(mode)
+    if convolve:
+        weights = weights[::-1]
+        origin = -origin
+        if K % 2 == 0:
+            origin -= 1
+    anchor = K // 2 + origin
+    wdt = weights_dtype(x.dtype, weights.dtype)
+    R = np.float64 if wdt == np.complex128 else np.float32
+    taps = weights.astype(wdt)
+    path = choose_path(x.ndim, axis, K, anchor, mode, cval, x.dtype, algorithm)
+    elementwise = path != "shared_memory"
+    # the fill value as W
+    if elementwise:
+        cre, cim = R(cval), R(0.0) if cval >= 0 else R(-0.0)
+    else:
+        t = x.dtype if x.dtype.kind != "c" else np.empty(0, x.dtype).real.dtype
+        if t.kind in "iu":
+            cre = R(_lib.oracle_cval_as_input(float(cval), _dchar(x.dtype), int(R == np.float64)))
+        else:
+            cre = R(np.asarray(cval).astype(t))
+        cim = R(0.0)
+    xs = np.moveaxis(x, axis, -1)
+    if x.dtype.kind == "c":
+        xr, xi = xs.real.astype(R), xs.imag.astype(R)
+    else:
+        xr = xs.astype(R)
+        neg = elementwise and mode != "constant" and x.dtype.kind == "f"
+        xi = np.where(~(xr >= 0), R(-0.0), R(0.0)).astype(R) if neg else np.zeros_like(xr)
+    L = xs.shape[-1]
+    pos = np.arange(L)
+    sr = np.zeros(xs.shape, R)
+    si = np.zeros(xs.shape, R)
+    for k in range(K):
+        wr, wi = R(taps[k].real), R(taps[k].imag)
+        if elementwise and wr == 0 and wi == 0:
+            continue
+        m = _map_coords(pos - anchor + k, L, mode)
+        inside = m >= 0
+        vr = np.where(inside, xr[..., np.maximum(m, 0)], cre).astype(R)
+        vi = np.where(inside, xi[..., np.maximum(m, 0)], cim).astype(R)
+        pr = fma(vr, wr, -(vi * wi))
+        pi = fma(vi, wr, vr * wi)
+        sr = (sr + pr).astype(R)
+        si = (si + pi).astype(R)
+    cdt = np.empty(0, out.dtype).real.dtype
+    res = np.empty(xs.shape, out.dtype)
+    res.real = sr.astype(cdt)
+    res.imag = si.astype(cdt)
+    out[...] = np.moveaxis(res, -1, axis)
+    return out
+
+
 def correlate1d(input, weights, axis=-1, output=None, mode="reflect", cval=0.0,
                 origin=0, *, algorithm=None, convolve=False):
     """FLT:135-178 / FLT:180-221 -> FLT:271-344."""
     input = np.asarray(input)
+    weights = np.asarray(weights)
+    if input.dtype.kind == "c" or weights.dtype.kind == "c":
+        axis = axis % input.ndim if input.ndim else 0
+        if weights.dtype.kind == "c" and not convolve:
+            weights = weights.conj()  # numpy.correlate conjugates the weights
+        out = get_output(output, input, complex_output=True)
+        return _complex_correlate1d(input, weights, axis, out, mode, cval, origin, algorithm,
+                                    convolve)
     axis = axis % input.ndim if input.ndim else 0
     params = pass_params(input.dtype, input.ndim, axis, weights, mode, cval, origin,
                          convolve, algorithm)

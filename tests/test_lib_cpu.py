@@ -61,7 +61,13 @@ def test_validation_happens_before_device_work():
     good_out = _arr((4, 5), np.float32, 0x9000)
     assert _corr(good_in, _arr((4, 6), np.float32, 0x9000)) == _lib.E_INVALID
     assert "shape" in _lib.last_error()
-    assert _corr(good_in, _arr((4, 5), np.complex64, 0x9000)) == _lib.E_DTYPE
+    assert _corr(good_in, _arr((4, 5), np.bool_, 0x9000)) == _lib.E_DTYPE
+    # complex input needs a complex output (refused before any device work)
+    assert _corr(_arr((4, 5), np.complex64, 0x1000), good_out) == _lib.E_DTYPE
+    assert "complex" in _lib.last_error()
+    # complex64 overlaps by its 8-byte elements
+    assert _corr(_arr((4, 5), np.complex64, 0x1000),
+                 _arr((4, 5), np.complex64, 0x1000 + 8 * 19)) == _lib.E_INVALID
     assert _corr(_arr((4, 5), np.float32, 0x1000, strides=(4, 16)), good_out) == _lib.E_LAYOUT
     assert _corr(good_in, good_out, K=3, origin=2) == _lib.E_INVALID
     assert "origin" in _lib.last_error()
@@ -211,3 +217,25 @@ def test_c_entries_reject_bad_arguments():
     rc = _lib.lib.cimx_uniform_nd(ctypes.byref(a), ctypes.byref(b), (ctypes.c_int * 2)(3, 3),
                                   modes, (ctypes.c_int * 2)(2, 0), None, 2, 0.0, 0, 0, None)
     assert rc == _lib.E_INVALID and "origin" in _lib.last_error()
+
+
+def test_complex_pass_list():
+    """Complex taps travel as (re, im) pairs with ntaps = their count, the
+    complex-taps flag set and W = complex<float> / complex<double> by cuCIM's
+    rule (UTIL:35-37)."""
+    from cucim_b200 import ndimage
+
+    w = np.array([0.2 + 0.1j, -0.5 + 0.3j, 0.0, 0.1 - 0.05j])
+    pl = ndimage._build_passes(np.dtype(np.complex64), np.dtype(np.complex64), 1,
+                               [(0, w, "reflect", 1, False)], 0.0, None)
+    p = pl.items[0]
+    assert p.ntaps == 4 and p.origin == 1
+    assert p.flags & _lib.F_COMPLEX_TAPS and not p.flags & _lib.F_W64
+    assert [p.taps[i] for i in range(8)] == [0.2, 0.1, -0.5, 0.3, 0.0, 0.0, 0.1, -0.05]
+    pl = ndimage._build_passes(np.dtype(np.int32), np.dtype(np.complex128), 2,
+                               [(1, np.ones(3), "reflect", 0, False)], 0.0, None)
+    p = pl.items[0]
+    assert p.ntaps == 3 and not p.flags & _lib.F_COMPLEX_TAPS
+    pl = ndimage._build_passes(np.dtype(np.complex128), np.dtype(np.complex128), 2,
+                               [(1, np.ones(3), "reflect", 0, False)], 0.0, None)
+    assert pl.items[0].flags & _lib.F_W64

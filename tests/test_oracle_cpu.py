@@ -163,6 +163,36 @@ def test_correlate1d_vs_scipy_f64(mode, K, convolve):
 
 
 @pytest.mark.parametrize("mode", MODES)
+@pytest.mark.parametrize("wkind", ["real", "complex"])
+@pytest.mark.parametrize("convolve", [False, True])
+def test_complex_correlate1d_vs_scipy_c128(mode, wkind, convolve):
+    """The complex restatement (complex128: W = complex<double>) against
+    scipy's complex correlate1d, including correlate's conjugated weights,
+    convolve's flip and K > n."""
+    rng = np.random.default_rng(11)
+    x = rng.standard_normal((7, 9, 11)) + 1j * rng.standard_normal((7, 9, 11))
+    w = rng.standard_normal(13)
+    if wkind == "complex":
+        w = w + 1j * rng.standard_normal(13)
+    f, g = (R.convolve1d, sndi.convolve1d) if convolve else (R.correlate1d, sndi.correlate1d)
+    for axis in range(3):
+        a = f(x, w, axis, mode=mode, cval=-0.5, origin=1)
+        b = g(x, w, axis, mode=mode, cval=-0.5, origin=1)
+        assert a.dtype == np.complex128
+        np.testing.assert_allclose(a, b, rtol=1e-12, atol=1e-12)
+
+
+def test_complex_real_input_complex_weights_vs_scipy():
+    rng = np.random.default_rng(12)
+    x = rng.standard_normal((20, 30)).astype(np.float32)
+    w = np.array([0.2 + 0.1j, 0.5 - 0.3j, 0.1 + 0.05j])
+    a = R.correlate1d(x, w, 1)
+    assert a.dtype == np.complex64
+    np.testing.assert_allclose(a, sndi.correlate1d(x.astype(np.float64), w, 1), rtol=0,
+                               atol=4e-7)
+
+
+@pytest.mark.parametrize("mode", MODES)
 def test_kernel_longer_than_axis_vs_scipy(mode):
     """Multi-period reflection when K > n (UTIL:186-308)."""
     x = np.random.default_rng(3).standard_normal((3, 4))
