@@ -15,12 +15,14 @@
 //   out   = sqrt(d0*d0 + d1*d1), each product and the sum rounded to float32.
 //
 // Work: the tiles' 64 x 64 output blocks form one flat list (each tile knows
-// the index of its first block); CTAs walk the list with a grid stride. A
-// block stages its gray halo region (64 + 2 + 2r)^2 in shared memory, runs
-// the y pass into a second buffer, then the x pass, the two edge passes and
-// the two smoothing passes in the space the gray region left. The launch
-// reads only device memory that the caller prepared, so it can be captured
-// in a CUDA graph and replayed.
+// the index of its first block); CTAs (three per SM up to a radius of about
+// 38) walk the list with a grid stride. A block computes its gray halo
+// region ((64 + 2 + 2r) rows) in strips of 28 columns through two
+// shared-memory buffers, the next strip's loads in flight during the current
+// strip's y pass into T; then the x pass into S (over the strip buffers),
+// and the edge, smoothing and magnitude steps per 4 outputs in registers.
+// The launch reads only device memory that the caller prepared, so it can
+// be captured in a CUDA graph and replayed.
 #include <algorithm>
 #include <mutex>
 
@@ -60,8 +62,23 @@ __device__ __forceinline__ float luma_f64(double r, double g, double b) {
 
 constexpr int kSS = kBT + 3;  // row stride of S: odd, for the column-wise writes of the x pass
 constexpr int kGB = 4;  // 4-pixel groups whose words a thread loads at once (gray step)
+constexpr int kCW = 28;  // gray-region columns per strip: 9 x 28 y-pass items fill 256 threads once
+constexpr int kCG = kCW / 4;  // 4-pixel groups per strip row
+constexpr int kSlack = 16;    // spare strip rows: the chains may read 2 x 8 - 1 rows past the last
 constexpr int kBR = 8;  // outputs per thread in the Gaussian passes
 constexpr int kBG = (kBT + 2 + kBR - 1) / kBR;  // 8-output groups over 66 rows or columns
+
+// Shared-memory areas for the batch's largest radius (floats). A: two gray
+// strips of (64 + 2 + 2 max_r + kSlack) rows x kCW, or S (66 x kSS). B: T
+// (66 rows x the odd stride 64 + 3 + 2 max_r, 64 spare floats for the x
+// chains' reads past the last row).
+__host__ __device__ inline int batch_area_a(int max_r) {
+  const int strips = 2 * (kBT + 2 + 2 * max_r + kSlack) * kCW;
+  return strips > (kBT + 2) * kSS ? strips : (kBT + 2) * kSS;
+}
+__host__ __device__ inline int batch_area_b(int max_r) {
+  return (kBT + 2) * (kBT + 3 + 2 * max_r) + 64;
+}
 
 // acc[p] = the fused multiply-add chain over taps k = 0 .. K-1 of
 // x(p + k) * w[k], for kBR consecutive outputs p: the taps ascending from
@@ -100,7 +117,7 @@ __device__ __forceinline__ void chain_r(float (&acc)[kBR], const float* w, int K
   }
 }
 
-__global__ void __launch_bounds__(kBThreads, 2) k_batch_gray_gauss_sobel(const BatchArgs a) {
+__global__ void __launch_bounds__(kBThreads, 3) k_batch_gray_gauss_sobel(const BatchArgs a) {
   extern __shared__ float smf[];
   __shared__ CimxBatchTile s_t;                    // this block's tile
   __shared__ float s_w[kBMaxTaps];                 // this tile's taps
@@ -109,16 +126,16 @@ __global__ void __launch_bounds__(kBThreads, 2) k_batch_gray_gauss_sobel(const B
   __shared__ double s_ch[256];                     // channel_f64 of every byte value
   const int tid = threadIdx.x;
   for (int u = tid; u < 256; u += kBThreads) s_ch[u] = channel_f64(u);
-  // strides sized for the batch's largest radius; odd, so that lanes on
-  // consecutive rows read different banks
-  const int gcs = kBT + 3 + 2 * a.max_r;  // row stride of the gray region and of T
-  float* G = smf;                          // (64 + 2 + 2r) rows x gcs
-  float* T = smf + gcs * gcs;              // 66 rows x gcs
-  // overlays of G once T exists: S (66 x 66, row stride kSS), E0 (64 x 66),
-  // E1 (66 x 64)
-  float* S = smf;
-  float* E0 = S + (kBT + 2) * kSS;
-  float* E1 = E0 + kBT * (kBT + 2);
+  // sizes for the batch's largest radius. Area A: two strip buffers of the
+  // gray region (kCW columns, kSlack spare rows for the register-blocked
+  // chains' reads past the last row), later S. Area B: T (odd row stride,
+  // so that lanes on consecutive rows read different banks).
+  const int gcs = kBT + 3 + 2 * a.max_r;
+  const int gsr = kBT + 2 + 2 * a.max_r + kSlack;
+  float* const Gb0 = smf;
+  float* const Gb1 = smf + gsr * kCW;
+  float* const T = smf + batch_area_a(a.max_r);
+  float* const S = smf;
 
   for (long long g = blockIdx.x; g < a.nblocks; g += gridDim.x) {
     if (tid < 32) {
@@ -181,91 +198,115 @@ __global__ void __launch_bounds__(kBThreads, 2) k_batch_gray_gauss_sobel(const B
       (tid < kBG ? s_yc : s_xc)[q] = ok;
     }
 
-    // 1. gray region: rows y0-1-r .., columns x0-1-r .., 'nearest' borders.
-    //    A thread takes groups of 4 consecutive pixels of a row: where they
-    //    lie inside the row, their 12 bytes come from three or four aligned
-    //    32-bit words (each word holds at least one of the 12 bytes, so it
-    //    lies in the tile's allocation); at the tile's borders pixel by
-    //    pixel. The words of kGB groups are loaded before any is used.
-    {
-      const int GC4 = (GC + 3) >> 2, ng = GR * GC4;
-      const int xb = x0 - 1 - r;  // source column of region column 0
-      for (int i0 = tid; i0 < ng; i0 += kGB * kBThreads) {
-        uint32_t wv[kGB][4];
-        unsigned shv[kGB];
-        bool fast[kGB];
+    // 1-2. the gray region (rows y0-1-r .., columns x0-1-r .., 'nearest'
+    //    borders) and the gaussian along y, in strips of kCW region columns
+    //    through two buffers: while the y pass runs on strip s, the words of
+    //    strip s + 1 are in flight. Gray: a thread takes groups of 4
+    //    consecutive pixels of a row; where they lie inside the row, their
+    //    12 bytes come from three or four aligned 32-bit words (each word
+    //    holds at least one of the 12 bytes, so it lies in the tile's
+    //    allocation), at the tile's borders pixel by pixel. The y pass: T
+    //    row tr is the smoothed row refl(y0 - 1 + tr) (rows outside the tile
+    //    only feed outputs that are not stored); a thread takes 8
+    //    consecutive T rows of one column, one by one where their source
+    //    rows are not consecutive (tile borders).
+    const int ng = GR * kCG;       // 4-pixel groups of one strip
+    const int xb = x0 - 1 - r;     // source column of region column 0
+    const int nstrips = (GC + kCW - 1) / kCW;
+    uint32_t wv[kGB][4];
+    unsigned shv[kGB];
+    bool fast[kGB];
+    auto gray_load = [&](int st, int i0) {
 #pragma unroll
-        for (int u = 0; u < kGB; ++u) {
-          const int idx = i0 + u * kBThreads;
-          const int gr = idx / GC4, c0 = (idx - gr * GC4) * 4;
+      for (int u = 0; u < kGB; ++u) {
+        const int idx = i0 + u * kBThreads;
+        const int gr = idx / kCG, c0 = st * kCW + (idx - gr * kCG) * 4;
+        const int xs = xb + c0;
+        fast[u] = idx < ng && c0 + 3 < GC && xs >= 0 && xs + 3 < W;
+        shv[u] = 0;
+        wv[u][0] = wv[u][1] = wv[u][2] = wv[u][3] = 0u;
+        if (fast[u]) {
+          const uint8_t* px = t.rgb + static_cast<long long>(nearest_idx(y0 - 1 - r + gr, H)) * in_pitch + 3LL * xs;
+          const uintptr_t pa = reinterpret_cast<uintptr_t>(px);
+          const uint32_t* wp = reinterpret_cast<const uint32_t*>(pa & ~static_cast<uintptr_t>(3));
+          shv[u] = static_cast<unsigned>(pa & 3) * 8u;
+          wv[u][0] = __ldg(wp);
+          wv[u][1] = __ldg(wp + 1);
+          wv[u][2] = __ldg(wp + 2);
+          if (shv[u]) wv[u][3] = __ldg(wp + 3);
+        }
+      }
+    };
+    auto gray_store = [&](int st, int i0) {
+      float* Gs = (st & 1) ? Gb1 : Gb0;
+#pragma unroll
+      for (int u = 0; u < kGB; ++u) {
+        const int idx = i0 + u * kBThreads;
+        if (idx >= ng) break;
+        const int gr = idx / kCG, cl = (idx - gr * kCG) * 4, c0 = st * kCW + cl;
+        if (c0 >= GC) continue;
+        float* dst = Gs + gr * kCW + cl;
+        if (fast[u]) {
+          const unsigned sh = shv[u];
+          const uint32_t v0 = __funnelshift_r(wv[u][0], wv[u][1], sh);
+          const uint32_t v1 = __funnelshift_r(wv[u][1], wv[u][2], sh);
+          const uint32_t v2 = __funnelshift_r(wv[u][2], wv[u][3], sh);
+          dst[0] = luma_f64(s_ch[v0 & 255u], s_ch[(v0 >> 8) & 255u], s_ch[(v0 >> 16) & 255u]);
+          dst[1] = luma_f64(s_ch[v0 >> 24], s_ch[v1 & 255u], s_ch[(v1 >> 8) & 255u]);
+          dst[2] = luma_f64(s_ch[(v1 >> 16) & 255u], s_ch[v1 >> 24], s_ch[v2 & 255u]);
+          dst[3] = luma_f64(s_ch[(v2 >> 8) & 255u], s_ch[(v2 >> 16) & 255u], s_ch[v2 >> 24]);
+        } else {
+          const uint8_t* row = t.rgb + static_cast<long long>(nearest_idx(y0 - 1 - r + gr, H)) * in_pitch;
           const int xs = xb + c0;
-          fast[u] = idx < ng && xs >= 0 && xs + 3 < W && c0 + 3 < GC;
-          shv[u] = 0;
-          wv[u][0] = wv[u][1] = wv[u][2] = wv[u][3] = 0u;
-          if (fast[u]) {
-            const uint8_t* px = t.rgb + static_cast<long long>(nearest_idx(y0 - 1 - r + gr, H)) * in_pitch + 3LL * xs;
-            const uintptr_t pa = reinterpret_cast<uintptr_t>(px);
-            const uint32_t* wp = reinterpret_cast<const uint32_t*>(pa & ~static_cast<uintptr_t>(3));
-            shv[u] = static_cast<unsigned>(pa & 3) * 8u;
-            wv[u][0] = __ldg(wp);
-            wv[u][1] = __ldg(wp + 1);
-            wv[u][2] = __ldg(wp + 2);
-            if (shv[u]) wv[u][3] = __ldg(wp + 3);
-          }
-        }
-#pragma unroll
-        for (int u = 0; u < kGB; ++u) {
-          const int idx = i0 + u * kBThreads;
-          if (idx >= ng) break;
-          const int gr = idx / GC4, c0 = (idx - gr * GC4) * 4;
-          float* dst = G + gr * gcs + c0;
-          if (fast[u]) {
-            const unsigned sh = shv[u];
-            const uint32_t v0 = __funnelshift_r(wv[u][0], wv[u][1], sh);
-            const uint32_t v1 = __funnelshift_r(wv[u][1], wv[u][2], sh);
-            const uint32_t v2 = __funnelshift_r(wv[u][2], wv[u][3], sh);
-            dst[0] = luma_f64(s_ch[v0 & 255u], s_ch[(v0 >> 8) & 255u], s_ch[(v0 >> 16) & 255u]);
-            dst[1] = luma_f64(s_ch[v0 >> 24], s_ch[v1 & 255u], s_ch[(v1 >> 8) & 255u]);
-            dst[2] = luma_f64(s_ch[(v1 >> 16) & 255u], s_ch[v1 >> 24], s_ch[v2 & 255u]);
-            dst[3] = luma_f64(s_ch[(v2 >> 8) & 255u], s_ch[(v2 >> 16) & 255u], s_ch[v2 >> 24]);
-          } else {
-            const uint8_t* row = t.rgb + static_cast<long long>(nearest_idx(y0 - 1 - r + gr, H)) * in_pitch;
-            const int xs = xb + c0;
-            for (int p = 0; p < 4 && c0 + p < GC; ++p) {
-              const uint8_t* px = row + 3LL * nearest_idx(xs + p, W);
-              dst[p] = luma_f64(s_ch[px[0]], s_ch[px[1]], s_ch[px[2]]);
-            }
+          for (int p = 0; p < 4 && c0 + p < GC; ++p) {
+            const uint8_t* px = row + 3LL * nearest_idx(xs + p, W);
+            dst[p] = luma_f64(s_ch[px[0]], s_ch[px[1]], s_ch[px[2]]);
           }
         }
       }
-    }
-    __syncthreads();
-
-    // 2. gaussian along y: T row tr is the smoothed row refl(y0 - 1 + tr);
-    //    rows outside the tile only feed outputs that are not stored. A
-    //    thread takes 8 consecutive T rows of one column; where their source
-    //    rows are not consecutive (tile borders) it runs them one by one.
-    for (int idx = tid; idx < kBG * GC; idx += kBThreads) {
-      const int q = idx / GC, c = idx - q * GC;
-      const int tr0 = q * kBR, nr = min(kBR, kBT + 2 - tr0);
-      if (s_yc[q]) {
-        float acc[kBR];
+    };
+    auto ypass = [&](int st) {
+      const float* Gs = (st & 1) ? Gb1 : Gb0;
+      for (int idx = tid; idx < kBG * kCW; idx += kBThreads) {
+        const int q = idx / kCW, cl = idx - q * kCW, c = st * kCW + cl;
+        if (c >= GC) continue;
+        const int tr0 = q * kBR, nr = min(kBR, kBT + 2 - tr0);
+        if (s_yc[q]) {
+          float acc[kBR];
 #pragma unroll
-        for (int p = 0; p < kBR; ++p) acc[p] = 0.f;
-        const float* col = G + (s_ci[tr0] - r) * gcs + c;
-        chain_r(acc, s_w, K, [&](int i) { return col[i * gcs]; });
+          for (int p = 0; p < kBR; ++p) acc[p] = 0.f;
+          const float* col = Gs + (s_ci[tr0] - r) * kCW + cl;
+          chain_r(acc, s_w, K, [&](int i) { return col[i * kCW]; });
 #pragma unroll
-        for (int p = 0; p < kBR; ++p) T[(tr0 + p) * gcs + c] = acc[p];
-      } else {
-        for (int p = 0; p < nr; ++p) {
-          const float* col = G + (s_ci[tr0 + p] - r) * gcs + c;
-          float acc = 0.f;
-          for (int k = 0; k < K; ++k) acc = fmaf(col[k * gcs], s_w[k], acc);
-          T[(tr0 + p) * gcs + c] = acc;
+          for (int p = 0; p < kBR; ++p) T[(tr0 + p) * gcs + c] = acc[p];
+        } else {
+          for (int p = 0; p < nr; ++p) {
+            const float* col = Gs + (s_ci[tr0 + p] - r) * kCW + cl;
+            float acc = 0.f;
+            for (int k = 0; k < K; ++k) acc = fmaf(col[k * kCW], s_w[k], acc);
+            T[(tr0 + p) * gcs + c] = acc;
+          }
         }
       }
+    };
+    for (int i0 = tid; i0 < ng; i0 += kGB * kBThreads) {
+      gray_load(0, i0);
+      gray_store(0, i0);
     }
     __syncthreads();
+    for (int st = 0; st < nstrips; ++st) {
+      const bool next = st + 1 < nstrips;  // the same for every thread
+      if (next) gray_load(st + 1, tid);
+      ypass(st);
+      if (next) {
+        gray_store(st + 1, tid);
+        for (int i0 = tid + kGB * kBThreads; i0 < ng; i0 += kGB * kBThreads) {
+          gray_load(st + 1, i0);
+          gray_store(st + 1, i0);
+        }
+      }
+      __syncthreads();
+    }
 
     // 3. gaussian along x: S(sr, sc) is the smoothed value at
     //    (refl(y0 - 1 + sr), refl(x0 - 1 + sc)); a thread takes 8
@@ -292,42 +333,53 @@ __global__ void __launch_bounds__(kBThreads, 2) k_batch_gray_gauss_sobel(const B
     }
     __syncthreads();
 
-    // 4. edge passes: E0 along y (64 x 66), E1 along x (66 x 64)
-    for (int idx = tid; idx < kBT * (kBT + 2); idx += kBThreads) {
-      const int y = idx / (kBT + 2), sc = idx - y * (kBT + 2);
-      float acc = 0.f;
-      acc = fmaf(S[y * kSS + sc], a.edge[0], acc);
-      acc = fmaf(S[(y + 1) * kSS + sc], a.edge[1], acc);
-      acc = fmaf(S[(y + 2) * kSS + sc], a.edge[2], acc);
-      E0[idx] = acc;
-    }
-    for (int idx = tid; idx < (kBT + 2) * kBT; idx += kBThreads) {
-      const int sr = idx / kBT, x = idx - sr * kBT;
-      const float* row = S + sr * kSS + x;
-      float acc = 0.f;
-      acc = fmaf(row[0], a.edge[0], acc);
-      acc = fmaf(row[1], a.edge[1], acc);
-      acc = fmaf(row[2], a.edge[2], acc);
-      E1[idx] = acc;
-    }
-    __syncthreads();
-
-    // 5. smoothing passes and the magnitude
-    for (int idx = tid; idx < kBT * kBT; idx += kBThreads) {
-      const int y = idx / kBT, x = idx - y * kBT;
+    // 4-5. edge passes (E0 along y, E1 along x), smoothing passes and the
+    //    magnitude, per 4 consecutive outputs of a row: every E0 and E1
+    //    value they read comes from the 3 x 6 window of S at (y, x), kept in
+    //    registers; each value is the same chain as a separate pass over a
+    //    stored E0 / E1 would compute. Lanes take consecutive rows (S's odd
+    //    row stride: conflict-free).
+    for (int it = tid; it < kBT * (kBT / 4); it += kBThreads) {
+      const int y = it % kBT, x = (it / kBT) * 4;
       if (y0 + y >= H || x0 + x >= W) continue;
-      const float* e0 = E0 + y * (kBT + 2) + x;
-      float d0 = 0.f;
-      d0 = fmaf(e0[0], a.smooth[0], d0);
-      d0 = fmaf(e0[1], a.smooth[1], d0);
-      d0 = fmaf(e0[2], a.smooth[2], d0);
-      const float* e1 = E1 + y * kBT + x;
-      float d1 = 0.f;
-      d1 = fmaf(e1[0], a.smooth[0], d1);
-      d1 = fmaf(e1[kBT], a.smooth[1], d1);
-      d1 = fmaf(e1[2 * kBT], a.smooth[2], d1);
-      const float m = __fadd_rn(__fmul_rn(d0, d0), __fmul_rn(d1, d1));
-      t.out[static_cast<long long>(y0 + y) * out_pitch + x0 + x] = sqrtf(m);
+      float sw[3][6];
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int c = 0; c < 6; ++c) sw[i][c] = S[(y + i) * kSS + x + c];
+      float e0[6], e1[3][4];
+#pragma unroll
+      for (int c = 0; c < 6; ++c) {
+        float acc = 0.f;
+        acc = fmaf(sw[0][c], a.edge[0], acc);
+        acc = fmaf(sw[1][c], a.edge[1], acc);
+        acc = fmaf(sw[2][c], a.edge[2], acc);
+        e0[c] = acc;
+      }
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          float acc = 0.f;
+          acc = fmaf(sw[i][c], a.edge[0], acc);
+          acc = fmaf(sw[i][c + 1], a.edge[1], acc);
+          acc = fmaf(sw[i][c + 2], a.edge[2], acc);
+          e1[i][c] = acc;
+        }
+      float* orow = t.out + static_cast<long long>(y0 + y) * out_pitch + x0 + x;
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        float d0 = 0.f;
+        d0 = fmaf(e0[c], a.smooth[0], d0);
+        d0 = fmaf(e0[c + 1], a.smooth[1], d0);
+        d0 = fmaf(e0[c + 2], a.smooth[2], d0);
+        float d1 = 0.f;
+        d1 = fmaf(e1[0][c], a.smooth[0], d1);
+        d1 = fmaf(e1[1][c], a.smooth[1], d1);
+        d1 = fmaf(e1[2][c], a.smooth[2], d1);
+        const float m = __fadd_rn(__fmul_rn(d0, d0), __fmul_rn(d1, d1));
+        if (x0 + x + c < W) orow[c] = sqrtf(m);
+      }
     }
     __syncthreads();  // shared buffers are reused by the next block
   }
@@ -358,14 +410,8 @@ extern "C" int cimx_batch_gray_gauss_sobel(const CimxBatchTile* tiles, int ntile
     a.edge[k] = edge_taps[k];
     a.smooth[k] = smooth_taps[k];
   }
-  // gray region + T, or S + E0 + E1 (which overlay the gray region and
-  // spill into T for small radii), whichever is larger
-  const int gcs = kBT + 3 + 2 * a.max_r;
-  // the register-blocked chains read up to 2 * 8 - 1 inputs past the last
-  // one they use: slack after T for its last row
-  const size_t region = static_cast<size_t>(gcs) * gcs + static_cast<size_t>(kBT + 2) * gcs + 64;
-  const size_t overlay = static_cast<size_t>(kBT + 2) * kSS + 2 * kBT * (kBT + 2);
-  const size_t smem = sizeof(float) * std::max(region, overlay);
+  const size_t smem = sizeof(float) * (static_cast<size_t>(batch_area_a(a.max_r)) +
+                                       static_cast<size_t>(batch_area_b(a.max_r)));
   // the kernel also holds about 3.2 KB of static shared memory (taps, the
   // row / column tables, the channel table); the sum stays under the 227 KB
   // per CTA
@@ -381,7 +427,14 @@ extern "C" int cimx_batch_gray_gauss_sobel(const CimxBatchTile* tiles, int ntile
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const long long grid = std::min<long long>(nblocks, 2LL * sms);
+  // resident CTAs per SM: three while the shared memory allows (largest
+  // radius up to about 38), two beyond; the grid walks the block list with
+  // a stride
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_gray_gauss_sobel, kBThreads,
+                                                    smem) != cudaSuccess || per_sm < 1)
+    per_sm = 1;
+  const long long grid = std::min<long long>(nblocks, static_cast<long long>(per_sm) * sms);
   k_batch_gray_gauss_sobel<<<(unsigned)grid, kBThreads, smem, static_cast<cudaStream_t>(stream)>>>(a);
   return cuda_fail(cudaGetLastError(), "batch launch");
 }
