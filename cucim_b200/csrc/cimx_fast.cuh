@@ -517,7 +517,11 @@ __global__ void __launch_bounds__(Geom<T, KB>::NT, Geom<T, KB>::MINB) k_slab(con
     tma_load_3d(reinterpret_cast<unsigned char*>(raw0) + k * G::RAWP, &map, bar + k,
                 static_cast<int>(xs), static_cast<int>(ys), static_cast<int>(bb));
   };
-  if (TMA && NBUF == 2 && threadIdx.x == 0 && blockIdx.z < a.B) issue(blockIdx.z, 0);
+  // float input, one buffer: the y pass is the last reader of the raw tile
+  // (the x pass reads s_mid), so the next slab's tile is issued right after
+  // it and lands while the x pass runs
+  constexpr bool kEarly = G::F32 && NBUF == 1;
+  if (TMA && (NBUF == 2 || kEarly) && threadIdx.x == 0 && blockIdx.z < a.B) issue(blockIdx.z, 0);
   long long it = 0;
   for (long long b = blockIdx.z; b < a.B; b += gridDim.z, ++it) {
   const T* in = static_cast<const T*>(a.in) + b * a.Y * a.X;
@@ -533,7 +537,7 @@ __global__ void __launch_bounds__(Geom<T, KB>::NT, Geom<T, KB>::MINB) k_slab(con
     int ok = 1;
     if (threadIdx.x == 0) {
       if (NBUF == 2 && b + gridDim.z < a.B) issue(b + gridDim.z, 1 - kb);
-      if (NBUF == 1) issue(b, 0);
+      if (NBUF == 1 && !kEarly) issue(b, 0);
       const uint32_t parity = static_cast<uint32_t>((it / NBUF) & 1);
       ok = mbar_wait(bar + kb, parity, a.status) ? 1 : 0;
     }
@@ -659,6 +663,8 @@ __global__ void __launch_bounds__(Geom<T, KB>::NT, Geom<T, KB>::MINB) k_slab(con
 
   if (a.has_x) {
     __syncthreads();
+    // every read of the raw tile is done: its next slab may land now
+    if (TMA && kEarly && threadIdx.x == 0 && b + gridDim.z < a.B) issue(b + gridDim.z, 0);
     // 3. x pass: one row pair x P consecutive outputs per item; output column
     //    g + q reads s_mid column g + q + sh, and since g is a multiple of 8,
     //    pad8(g + q + sh) = pad8(g) + pad8(q + sh)
@@ -696,6 +702,8 @@ __global__ void __launch_bounds__(Geom<T, KB>::NT, Geom<T, KB>::MINB) k_slab(con
     }
   }
   __syncthreads();  // shared buffers are reused by the next slab
+  if (TMA && kEarly && !a.has_x && threadIdx.x == 0 && b + gridDim.z < a.B)
+    issue(b + gridDim.z, 0);
   }
 }
 
@@ -719,13 +727,21 @@ int launch_slab_kb(SlabArgs& a, cudaStream_t st) {
   const bool tma = make_tensor_map_3d(&map, a.in, dt_code<T>(), a.X, a.Y, a.B, G::BX, G::BY);
   // without TMA a float tile is staged by plain loads into the raw buffer
   if (a.tiles_y > 65535) return CIMX_FUSED_DECLINED;
-  // enough CTAs to fill the GPU a few times; each walks a stride of slabs so
-  // that it can prefetch the next slab's tile while computing the current one
+  // enough CTAs to fill the GPU several times over; each walks a stride of
+  // slabs so that it can load the next slab's tile while computing the
+  // current one (float input: about four slabs per CTA, at least ~12 CTAs
+  // per SM)
   const long long per_slab = a.tiles_x * a.tiles_y;
-  const long long zs =
-      G::NBUF == 2 ? std::max<long long>(1, std::min<long long>(
-                                                {a.B, 65535LL, (148LL * 8 + per_slab - 1) / per_slab}))
-                   : std::min<long long>(a.B, 65535LL);
+  long long zs;
+  if (G::NBUF == 2)
+    zs = std::max<long long>(
+        1, std::min<long long>({a.B, 65535LL, (148LL * 8 + per_slab - 1) / per_slab}));
+  else if (G::F32 && tma)
+    zs = std::max<long long>(1, std::min<long long>({a.B, 65535LL,
+                                                     std::max<long long>((a.B + 3) / 4,
+                                                     (148LL * 12 + per_slab - 1) / per_slab)}));
+  else
+    zs = std::min<long long>(a.B, 65535LL);
   const dim3 grid((unsigned)a.tiles_x, (unsigned)a.tiles_y, (unsigned)zs);
   if (tma)
     k_slab<T, D, KB, true><<<grid, G::NT, G::SMEM, st>>>(map, a);
