@@ -46,6 +46,7 @@ L_NO_STREAM = 1 << 5
 L_NO_ROWSTREAM = 1 << 6
 L_NO_TUNE = 1 << 7
 L_ZCHUNK_SHIFT = 8
+L_SLAB_SPAN_SHIFT = 10
 
 E_INVALID, E_DTYPE, E_CUDA, E_NOMEM, E_LAYOUT, E_TIMEOUT = -1, -2, -3, -4, -5, -6
 

@@ -736,6 +736,8 @@ int launch_slab_kb(SlabArgs& a, cudaStream_t st) {
   if (G::NBUF == 2)
     zs = std::max<long long>(
         1, std::min<long long>({a.B, 65535LL, (148LL * 8 + per_slab - 1) / per_slab}));
+  else if (G::F32 && tma && a.span > 0)  // a tuned or forced span (any span is exact)
+    zs = std::max<long long>(1, std::min<long long>({a.B, 65535LL, (a.B + a.span - 1) / a.span}));
   else if (G::F32 && tma)
     zs = std::max<long long>(1, std::min<long long>({a.B, 65535LL,
                                                      std::max<long long>((a.B + 3) / 4,

@@ -226,6 +226,8 @@ int try_fused(const CimxArray* in, const CimxArray* out, PassDesc* ds, int npass
   if (rc == CIMX_OK && !tail.empty()) {
     SlabArgs a{};
     a.no_rowstream = (lib_flags & CIMX_L_NO_ROWSTREAM) ? 1 : 0;
+    static const int kSpans[4] = {0, 1, 2, 8};
+    a.span = kSpans[(lib_flags >> CIMX_L_SLAB_SPAN_SHIFT) & 3];
     a.in = src;
     a.out = dst_of(j++);
     a.X = in->shape[nd - 1];

@@ -30,6 +30,7 @@ struct SlabArgs {
   int has_y, has_x;
   int* status;  // device status word for bounded waits
   int no_rowstream;  // CIMX_L_NO_ROWSTREAM: always the slab kernel
+  int span;          // slabs per CTA (float input with TMA); 0: about four
   SlabPass py, px;
 };
 

@@ -334,7 +334,8 @@ void read_cache_once() {
 }
 
 constexpr int kScheduleBits = CIMX_L_NO_FUSION | CIMX_L_NO_VOLUME | CIMX_L_NO_STREAM |
-                              CIMX_L_NO_ROWSTREAM | (3 << CIMX_L_ZCHUNK_SHIFT);
+                              CIMX_L_NO_ROWSTREAM | (3 << CIMX_L_ZCHUNK_SHIFT) |
+                              (3 << CIMX_L_SLAB_SPAN_SHIFT);
 constexpr int kTensorBits = CIMX_L_TENSOR_BF16X3 | CIMX_L_TENSOR_TF32X3;
 
 }  // namespace
@@ -390,7 +391,10 @@ int tuned_flags(const std::string& key, int lib_flags, cudaStream_t st,
                        CIMX_L_NO_FUSION,
                        1 << CIMX_L_ZCHUNK_SHIFT,
                        2 << CIMX_L_ZCHUNK_SHIFT,
-                       3 << CIMX_L_ZCHUNK_SHIFT};
+                       3 << CIMX_L_ZCHUNK_SHIFT,
+                       1 << CIMX_L_SLAB_SPAN_SHIFT,
+                       2 << CIMX_L_SLAB_SPAN_SHIFT,
+                       3 << CIMX_L_SLAB_SPAN_SHIFT};
   for (int s : sched) cands.push_back(base | s);
   if (base & kTensorBits) {
     cands.push_back(base | CIMX_L_TENSOR_ALL_LINES);

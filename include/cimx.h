@@ -99,6 +99,8 @@ enum {
   CIMX_L_NO_TUNE = 1 << 7,      /* this call neither consults nor fills the tuning table */
   CIMX_L_ZCHUNK_SHIFT = 8,      /* bits 8-9: volume-kernel z chunk, 0 = automatic,
                                    1/2/3 = 32/64/128 slices */
+  CIMX_L_SLAB_SPAN_SHIFT = 10,  /* bits 10-11: slabs each slab-kernel CTA walks (float
+                                   input), 0 = automatic (about 4), 1/2/3 = 1/2/8 */
 };
 
 /* One 1-D correlation pass of a separable filter. */

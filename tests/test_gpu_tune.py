@@ -1,7 +1,8 @@
 """The autotuner on the GPU: tuning a call signature records one table
 entry, and the result of the tuned schedule is bit-identical to the oracle
 and to every forced schedule (volume kernel or not, stream or generic
-leading passes, row stream or slab, z chunks, one launch per pass). A later
+leading passes, row stream or slab, z chunks, slabs per CTA, one launch
+per pass). A later
 call of the same signature uses the entry without timing again. With
 algorithm="tensor" the tuner may also pick the plain passes; either result
 stays within the tensor path's tolerance."""
@@ -24,10 +25,11 @@ def mods(cuda):
 
 
 def _schedules(lib):
-    z = lib.L_ZCHUNK_SHIFT
+    z, sp = lib.L_ZCHUNK_SHIFT, lib.L_SLAB_SPAN_SHIFT
     return [lib.L_NO_FUSION, lib.L_NO_VOLUME, lib.L_NO_ROWSTREAM, lib.L_NO_STREAM,
             lib.L_NO_VOLUME | lib.L_NO_ROWSTREAM, lib.L_NO_VOLUME | lib.L_NO_STREAM,
-            1 << z, 2 << z, 3 << z]
+            1 << z, 2 << z, 3 << z, 1 << sp, 2 << sp, 3 << sp,
+            lib.L_NO_VOLUME | lib.L_NO_ROWSTREAM | (3 << sp)]
 
 
 def _u16(shape, seed):
