@@ -605,11 +605,25 @@ def run_tiles(torch, dev, reps=3, check=64, n_tiles=4096):
     cpu_s = time.perf_counter() - t0
     spx = sum(h.shape[0] * h.shape[1] for h in host)
     oracle_ok = all(np.array_equal(b.outputs[i].cpu().numpy(), e) for i, e in zip(sample, exp))
+    # compute roofline: the useful float32 FMAs of the path per output pixel
+    # (K taps of each Gaussian pass, 3 + 3 taps of each sobel direction);
+    # the halo the kernel recomputes around every 64 x 64 block is not useful work
+    fma = 0
+    for t, sg in zip(tiles, sigmas):
+        K = 2 * int(4.0 * sg + 0.5) + 1
+        fma += int(t.shape[0]) * int(t.shape[1]) * (2 * K + 12)
+    fp32_nominal = 148 * 128 * 2 * 1.965e9 / 1e12
+    useful_tflops = 2 * fma / (ms_b * 1e-3) / 1e12
     return {"workload": f"{len(tiles)} uint8 RGB tiles, sides 64..1024 (seed 3), "
                         "rgb2gray -> gaussian(sigma 0.5..8, nearest) -> sobel magnitude, float32 out",
             "pixels": npx, "batched_ms": ms_b, "batched_gpx_s": npx / (ms_b * 1e-3) / 1e9,
             "per_tile_ms": ms_t, "per_tile_gpx_s": npx / (ms_t * 1e-3) / 1e9,
             "speedup": ms_t / ms_b, "launches_batched": 1, "launches_per_tile": "about 7 per tile",
+            "roofline": {"bound": "fp32", "achieved": useful_tflops, "peak": fp32_nominal,
+                         "unit": "TFLOP/s", "frac": useful_tflops / fp32_nominal,
+                         "note": "useful float32 FMAs (2K + 12 per output pixel) over the nominal "
+                                 "148 SM x 128 FMA/clk x 1.965 GHz; HBM traffic is 7 B per pixel "
+                                 f"({7 * npx / (ms_b * 1e-3) / 1e9:.0f} GB/s)"},
             "bit_identical": bool(same), "tiles_compared": len(range(0, len(tiles), step)),
             "oracle_bit_exact": bool(oracle_ok), "oracle_tiles_compared": len(sample),
             "cpu_baseline": {"value": spx / cpu_s / 1e9, "unit": "Gpx/s", "cores": R.THREADS,
