@@ -6,7 +6,7 @@
 // _shared/filters.py:21-166, filters/edges.py:148-306), computed with exactly
 // the arithmetic of the per-tile path of this library:
 //   gray  = (float)(0.0721 b + (0.2125 r + 0.7154 g)) in float64 fused multiply-adds,
-//           r = (float)u8 * (float)(1/255) (a 256-entry table of the float64 values);
+//           r = (float)u8 * (float)(1/255) widened to float64;
 //   T     = gaussian along y of gray (float32 FMA chain, taps ascending, from +0),
 //   S     = gaussian along x of T, both with 'nearest' borders;
 //   d0    = smooth along x of (edge along y of S), d1 = smooth along y of (edge along x of S),
@@ -48,9 +48,17 @@ struct BatchArgs {
 
 __device__ __forceinline__ int nearest_idx(int i, int n) { return i < 0 ? 0 : (i >= n ? n - 1 : i); }
 
-// The float64 value of one channel: (double)((float)u * (float)(1/255)).
-__device__ __forceinline__ double channel_f64(int u) {
-  return static_cast<double>(__fmul_rn(static_cast<float>(u), static_cast<float>(1.0 / 255.0)));
+// The float64 value of one channel, (double)((float)u * (float)(1/255)),
+// computed without a table (a table's random reads conflicted on the
+// shared-memory banks): float(u) exactly, the float32 product, then the
+// float widened by rebiasing its exponent (the value is 0 or normal)
+__device__ __forceinline__ double chan(uint32_t u) {
+  const float f = __fmul_rn(__fsub_rn(__uint_as_float(0x4B000000u | u), 8388608.0f),
+                            static_cast<float>(1.0 / 255.0));
+  const unsigned long long b = __float_as_uint(f);
+  return __longlong_as_double(
+      b ? static_cast<long long>((b << 29) + (static_cast<unsigned long long>(1023 - 127) << 52))
+        : 0ll);
 }
 
 // gray = (float)(0.2125 r + 0.7154 g + 0.0721 b) with the float64
@@ -123,9 +131,7 @@ __global__ void __launch_bounds__(kBThreads, 3) k_batch_gray_gauss_sobel(const B
   __shared__ float s_w[kBMaxTaps];                 // this tile's taps
   __shared__ int s_ci[kBT + 2], s_cj[kBT + 2];     // source row / column of each T row, S column
   __shared__ int s_yc[kBG], s_xc[kBG];             // group of 8 with consecutive sources
-  __shared__ double s_ch[256];                     // channel_f64 of every byte value
   const int tid = threadIdx.x;
-  for (int u = tid; u < 256; u += kBThreads) s_ch[u] = channel_f64(u);
   // sizes for the batch's largest radius. Area A: two strip buffers of the
   // gray region (kCW columns, kSlack spare rows for the register-blocked
   // chains' reads past the last row), later S. Area B: T (odd row stride,
@@ -251,16 +257,19 @@ __global__ void __launch_bounds__(kBThreads, 3) k_batch_gray_gauss_sobel(const B
           const uint32_t v0 = __funnelshift_r(wv[u][0], wv[u][1], sh);
           const uint32_t v1 = __funnelshift_r(wv[u][1], wv[u][2], sh);
           const uint32_t v2 = __funnelshift_r(wv[u][2], wv[u][3], sh);
-          dst[0] = luma_f64(s_ch[v0 & 255u], s_ch[(v0 >> 8) & 255u], s_ch[(v0 >> 16) & 255u]);
-          dst[1] = luma_f64(s_ch[v0 >> 24], s_ch[v1 & 255u], s_ch[(v1 >> 8) & 255u]);
-          dst[2] = luma_f64(s_ch[(v1 >> 16) & 255u], s_ch[v1 >> 24], s_ch[v2 & 255u]);
-          dst[3] = luma_f64(s_ch[(v2 >> 8) & 255u], s_ch[(v2 >> 16) & 255u], s_ch[v2 >> 24]);
+          // one 16-byte store: strip rows are 28 floats and groups start at
+          // multiples of 4, so dst is 16-byte aligned
+          *reinterpret_cast<float4*>(dst) = make_float4(
+              luma_f64(chan(v0 & 255u), chan((v0 >> 8) & 255u), chan((v0 >> 16) & 255u)),
+              luma_f64(chan(v0 >> 24), chan(v1 & 255u), chan((v1 >> 8) & 255u)),
+              luma_f64(chan((v1 >> 16) & 255u), chan(v1 >> 24), chan(v2 & 255u)),
+              luma_f64(chan((v2 >> 8) & 255u), chan((v2 >> 16) & 255u), chan(v2 >> 24)));
         } else {
           const uint8_t* row = t.rgb + static_cast<long long>(nearest_idx(y0 - 1 - r + gr, H)) * in_pitch;
           const int xs = xb + c0;
           for (int p = 0; p < 4 && c0 + p < GC; ++p) {
             const uint8_t* px = row + 3LL * nearest_idx(xs + p, W);
-            dst[p] = luma_f64(s_ch[px[0]], s_ch[px[1]], s_ch[px[2]]);
+            dst[p] = luma_f64(chan(px[0]), chan(px[1]), chan(px[2]));
           }
         }
       }
@@ -412,9 +421,8 @@ extern "C" int cimx_batch_gray_gauss_sobel(const CimxBatchTile* tiles, int ntile
   }
   const size_t smem = sizeof(float) * (static_cast<size_t>(batch_area_a(a.max_r)) +
                                        static_cast<size_t>(batch_area_b(a.max_r)));
-  // the kernel also holds about 3.2 KB of static shared memory (taps, the
-  // row / column tables, the channel table); the sum stays under the 227 KB
-  // per CTA
+  // the kernel also holds about 1.2 KB of static shared memory (taps, the
+  // row / column tables); the sum stays under the 227 KB per CTA
   constexpr int kDynLimit = 223 * 1024;
   if (smem > static_cast<size_t>(kDynLimit)) return fail(CIMX_E_INVALID, "batch: taps too long");
   static std::once_flag once;
