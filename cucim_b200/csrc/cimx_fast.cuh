@@ -701,7 +701,11 @@ __global__ void __launch_bounds__(Geom<T, KB>::NT, Geom<T, KB>::MINB) k_slab(con
       }
     }
   }
-  __syncthreads();  // shared buffers are reused by the next slab
+  // shared buffers are reused by the next slab. With float input, TMA and an
+  // x pass the barrier after the next slab's tile wait already orders this
+  // slab's x pass (the last reader of s_mid) before the next y pass, and the
+  // raw tile is not shared with s_mid: no barrier here
+  if (!(TMA && kEarly && a.has_x)) __syncthreads();
   if (TMA && kEarly && !a.has_x && threadIdx.x == 0 && b + gridDim.z < a.B)
     issue(b + gridDim.z, 0);
   }

@@ -44,11 +44,14 @@
 namespace cimx {
 namespace vol {
 
-// 16 warps per CTA, one CTA per SM; region rows per warp: 4 for 3 taps,
-// 3 for 5 taps (the ring of five slices needs the registers). Measured on a
-// 512 x 1024 x 1024 uint16 stack, 24 or 32 warps with fewer rows each ran
-// slower (register spills, more halo rows).
-constexpr int kNW = 16;
+// 16 warps per SM; region rows per warp: 4 for 3 taps, 3 for 5 taps (the
+// ring of five slices needs the registers). 3 taps: two CTAs of 8 warps per
+// SM (their barriers are independent; sobel on the 512 x 1024 x 1024 uint16
+// stack 0.922 against 0.957 ms with one CTA of 16); 5 taps: one CTA of 16
+// (the uniform filter 1.341 against 1.408 ms with two of 8). 24 or 32 warps
+// with fewer rows each ran slower (register spills, more halo rows).
+constexpr int kNW3 = 8;
+constexpr int kNW5 = 16;
 constexpr int kM3 = 4;
 constexpr int kM5 = 3;
 constexpr int kRX = 128;             // region columns (4 per lane)
@@ -137,7 +140,7 @@ __device__ __forceinline__ float pick4(const float (&v)[4], int e) {
 // skipped tap keeps inf and nan out of the chain). Without it every tap takes
 // part: for finite inputs a zero tap leaves an FMA chain from +0 unchanged.
 template <class T, class D, int K, int M, int NW, bool MASK, bool TRUNC>
-__global__ void __launch_bounds__(32 * NW, 1) k_vol(const VolKArgs<K> a) {
+__global__ void __launch_bounds__(32 * NW, NW <= 8 ? 2 : 1) k_vol(const VolKArgs<K> a) {
   constexpr int RY = vol_ry<K, M, NW>();
   constexpr int TYO = vol_out_rows<K, M, NW>();
   constexpr int RXH = K / 2;  // x halo used by the x chain (symmetric taps)
@@ -371,7 +374,7 @@ int launch_vol_km(const VolArgs& v, cudaStream_t st) {
   a.tiles_x = static_cast<int>((v.X + kTX - 1) / kTX);
   const long long tiles = (long long)a.tiles_x * ((v.Y + TY - 1) / TY);
   // z chunk: long enough that the K - 1 extra slices stay a small share,
-  // short enough for a few waves of CTAs (one per SM). Measured on the
+  // short enough for a few waves of CTAs (one or two per SM). Measured on the
   // 512 x 1024 x 1024 uint16 stack: 3 taps ran 2.3 % faster with 32-slice
   // chunks (12 waves) than with 64; 5 taps showed no such gain.
   const long long waves = K == 3 ? 12 : 6;
@@ -448,20 +451,20 @@ int launch_vol_td(const VolArgs& v, cudaStream_t st) {
   }
   if constexpr (sizeof(T) == 4) {
     if (mask) {
-      if (K == 3) return launch_vol_km<T, D, 3, kM3, kNW, true, false>(v, st);
-      if (K == 5) return launch_vol_km<T, D, 5, kM5, kNW, true, false>(v, st);
+      if (K == 3) return launch_vol_km<T, D, 3, kM3, kNW3, true, false>(v, st);
+      if (K == 5) return launch_vol_km<T, D, 5, kM5, kNW5, true, false>(v, st);
       return CIMX_FUSED_DECLINED;
     }
   }
   if constexpr (sizeof(T) < 4 && sizeof(D) < 4) {
     if (trunc_bounded<T, D>(v)) {
-      if (K == 3) return launch_vol_km<T, D, 3, kM3, kNW, false, true>(v, st);
-      if (K == 5) return launch_vol_km<T, D, 5, kM5, kNW, false, true>(v, st);
+      if (K == 3) return launch_vol_km<T, D, 3, kM3, kNW3, false, true>(v, st);
+      if (K == 5) return launch_vol_km<T, D, 5, kM5, kNW5, false, true>(v, st);
       return CIMX_FUSED_DECLINED;
     }
   }
-  if (K == 3) return launch_vol_km<T, D, 3, kM3, kNW, false, false>(v, st);
-  if (K == 5) return launch_vol_km<T, D, 5, kM5, kNW, false, false>(v, st);
+  if (K == 3) return launch_vol_km<T, D, 3, kM3, kNW3, false, false>(v, st);
+  if (K == 5) return launch_vol_km<T, D, 5, kM5, kNW5, false, false>(v, st);
   return CIMX_FUSED_DECLINED;
 }
 
