@@ -173,17 +173,19 @@ def output_slot(output, input_obj, input_t, shape=None, dtype=None):
 
     `dtype` is the default output dtype (the input's when None).
     """
-    shape = tuple(input_t.shape) if shape is None else tuple(shape)
+    shape = input_t.shape if shape is None else tuple(shape)
     if output is None:
-        dt = np_dtype(input_t) if dtype is None else np.dtype(dtype)
-        t = empty(shape, dt, input_t.device)
+        tdt = input_t.dtype if dtype is None else torch_dtype(dtype)
+        t = torch.empty(shape, dtype=tdt, device=input_t.device)
+        return OutputSlot(t, t, like=input_obj)
+    if isinstance(output, torch.dtype):
+        t = torch.empty(shape, dtype=output, device=input_t.device)
         return OutputSlot(t, t, like=input_obj)
     if is_dtype_like(output):
-        dt = np_dtype(output) if isinstance(output, torch.dtype) else np.dtype(output)
-        t = empty(shape, dt, input_t.device)
+        t = empty(shape, np.dtype(output), input_t.device)
         return OutputSlot(t, t, like=input_obj)
     out_t = as_tensor(output)
-    if tuple(out_t.shape) != shape:
+    if out_t.shape != shape:
         raise RuntimeError("output shape not correct")
     if out_t.is_contiguous() and not shares_memory(out_t, input_t):
         return OutputSlot(out_t, out_t, user=output)

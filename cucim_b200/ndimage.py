@@ -209,12 +209,13 @@ def _run(input, specs, output, cval, algorithm=None, cache_key=None, complex_wei
     lib_flags = _EXTRA_LIB_FLAGS
     if algorithm in _TENSOR_FLAGS:
         lib_flags, algorithm = lib_flags | _TENSOR_FLAGS[algorithm], None
-    in_dt = _arrays.np_dtype(xc)
     key = None
     if cache_key is not None:
-        key = (cache_key, in_dt.str, np.dtype(out_dt).str, xc.dim(), _hashable(cval), algorithm)
+        # torch dtypes stand for the numpy ones here (one-to-one, and cheaper)
+        key = (cache_key, xc.dtype, slot.work.dtype, xc.dim(), _hashable(cval), algorithm)
     hit = _PASS_CACHE.get(key) if key is not None else None
     if hit is None:
+        in_dt = _arrays.np_dtype(xc)
         pl = _build_passes(in_dt, out_dt, xc.dim(), specs() if callable(specs) else specs, cval,
                            algorithm)
         hit = (pl, pl.array(), len(pl))

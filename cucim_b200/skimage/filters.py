@@ -35,9 +35,14 @@ def gaussian(image, sigma=1, mode="nearest", cval=0, preserve_range=False, trunc
         axes = tuple(ax for ax in range(x.dim()) if ax != channel_axis % x.dim())
     else:
         axes = tuple(range(x.dim()))
-    image_f = _u.convert_to_float(image, preserve_range)
-    fdt = supported_float_type(_arrays.np_dtype(_arrays.as_tensor(image_f)))
-    image_f = _u.astype(image_f, fdt)
+    if x.dtype in (torch.float32, torch.float64):
+        # already its own supported float type: convert_to_float and astype
+        # leave it as it is
+        image_f, fdt = image, x.dtype
+    else:
+        image_f = _u.convert_to_float(image, preserve_range)
+        fdt = supported_float_type(_arrays.np_dtype(_arrays.as_tensor(image_f)))
+        image_f = _u.astype(image_f, fdt)
     if out is None:
         return ndi.gaussian_filter(image_f, sigma, output=fdt, mode=mode, cval=cval,
                                    truncate=truncate, axes=axes)
