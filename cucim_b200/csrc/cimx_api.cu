@@ -267,7 +267,7 @@ int cimx_separable(const CimxArray* in, const CimxArray* out, const CimxPass* pa
   if (n == 0) return CIMX_OK;
 
   // the autotuner's schedule for this signature (or the caller's flags)
-  if (!(lib_flags & CIMX_L_NO_TUNE)) {
+  if (!(lib_flags & CIMX_L_NO_TUNE) && tuning_needed(lib_flags)) {
     const std::string key = tune_key(in, out, ds.data(), npasses, lib_flags);
     lib_flags = tuned_flags(key, lib_flags, st, [&](int f) {
       return cimx_separable(in, out, passes, npasses, f, stream);

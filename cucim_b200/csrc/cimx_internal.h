@@ -59,6 +59,10 @@ void scratch_free(void* p, size_t nbytes, cudaStream_t s);
 // the library flags to run it with (the caller's, or the tuned schedule;
 // with tuning on and an unseen key, `run(flags)` is timed for every
 // candidate schedule first).
+// Whether a call with these flags consults the tuning table at all (tuning
+// on, or entries recorded and no schedule forced): cheap, so that untuned
+// calls skip building the key.
+bool tuning_needed(int lib_flags);
 std::string tune_key(const CimxArray* in, const CimxArray* out, const PassDesc* ds,
                      int npasses, int lib_flags);
 int tuned_flags(const std::string& key, int lib_flags, cudaStream_t st,

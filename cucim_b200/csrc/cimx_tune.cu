@@ -23,7 +23,9 @@
 // CIMX_TUNE_CACHE names a JSON file that is read at first use and rewritten
 // after every newly tuned signature.
 #include <algorithm>
+#include <atomic>
 #include <cctype>
+#include <charconv>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -60,6 +62,8 @@ struct DeviceTable {
 };
 std::mutex g_tables_mu;
 std::map<std::string, DeviceTable*> g_tables;  // never freed: lives until exit
+std::atomic<long long> g_entries{0};           // entries in all tables
+DeviceTable* g_dev_table[kMaxDev] = {};         // the current device's table, by index (g_tables_mu)
 
 std::mutex g_name_mu;
 std::string g_names[kMaxDev];
@@ -81,6 +85,20 @@ DeviceTable& table_for(const std::string& device) {
   DeviceTable*& t = g_tables[device];
   if (!t) t = new DeviceTable();
   return *t;
+}
+
+// the current device's table, found by name once per device index
+DeviceTable& current_table() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDev) return table_for("unknown");
+  {
+    std::lock_guard<std::mutex> g(g_tables_mu);
+    if (g_dev_table[dev]) return *g_dev_table[dev];
+  }
+  DeviceTable& t = table_for(device_name());
+  std::lock_guard<std::mutex> g(g_tables_mu);
+  g_dev_table[dev] = &t;
+  return t;
 }
 
 // ------------------------------------------------------------------ JSON
@@ -280,7 +298,7 @@ int load_text(const std::string& text, const char* what) {
           en.candidates.emplace_back((int)c.arr[0].num, c.arr[1].num);
     DeviceTable& t = table_for(dev->second.str);
     std::lock_guard<std::mutex> g(t.mu);
-    t.entries[key->second.str] = en;
+    if (t.entries.insert_or_assign(key->second.str, en).second) ++g_entries;
   }
   return CIMX_OK;
 }
@@ -342,15 +360,52 @@ constexpr int kTensorBits = CIMX_L_TENSOR_BF16X3 | CIMX_L_TENSOR_TF32X3;
 
 std::string tune_key(const CimxArray* in, const CimxArray* out, const PassDesc* ds,
                      int npasses, int lib_flags) {
-  std::ostringstream o;
-  o << (char)in->dtype << ">" << (char)out->dtype << " [";
-  for (int d = 0; d < in->ndim; ++d) o << (d ? "," : "") << in->shape[d];
-  o << "]";
-  for (int i = 0; i < npasses; ++i)
-    o << " a" << ds[i].axis << "k" << ds[i].K << "o" << ds[i].anchor << "m" << ds[i].mode
-      << (ds[i].w64 ? "d" : "") << (ds[i].skip_zero ? "z" : "") << (ds[i].cval_as_input ? "c" : "");
-  o << " t" << (lib_flags & (kTensorBits | CIMX_L_TENSOR_ALL_LINES));
-  return o.str();
+  // built with plain appends: this runs on every call that may be tuned
+  std::string o;
+  o.reserve(48 + 24 * npasses);
+  char b[24];
+  auto num = [&](long long v) {
+    const auto r = std::to_chars(b, b + sizeof(b), v);
+    o.append(b, r.ptr);
+  };
+  o += (char)in->dtype;
+  o += '>';
+  o += (char)out->dtype;
+  o += " [";
+  for (int d = 0; d < in->ndim; ++d) {
+    if (d) o += ',';
+    num(in->shape[d]);
+  }
+  o += ']';
+  for (int i = 0; i < npasses; ++i) {
+    o += " a";
+    num(ds[i].axis);
+    o += 'k';
+    num(ds[i].K);
+    o += 'o';
+    num(ds[i].anchor);
+    o += 'm';
+    num(ds[i].mode);
+    if (ds[i].w64) o += 'd';
+    if (ds[i].skip_zero) o += 'z';
+    if (ds[i].cval_as_input) o += 'c';
+  }
+  o += " t";
+  num(lib_flags & (kTensorBits | CIMX_L_TENSOR_ALL_LINES));
+  return o;
+}
+
+bool tuning_needed(int lib_flags) {
+  init_from_env();
+  int mode;
+  {
+    std::lock_guard<std::mutex> g(g_mode_mu);
+    mode = g_mode;
+  }
+  if (mode == CIMX_TUNE_OFF || (lib_flags & (kScheduleBits | CIMX_L_NO_TUNE))) return false;
+  if (mode == CIMX_TUNE_ON) return true;
+  read_cache_once();
+  return g_entries.load(std::memory_order_relaxed) > 0;  // nothing recorded: nothing to apply
 }
 
 int tuned_flags(const std::string& key, int lib_flags, cudaStream_t st,
@@ -364,7 +419,7 @@ int tuned_flags(const std::string& key, int lib_flags, cudaStream_t st,
   // a caller that chose a schedule, or asked for none to be tuned, keeps it
   if (mode == CIMX_TUNE_OFF || (lib_flags & (kScheduleBits | CIMX_L_NO_TUNE))) return lib_flags;
   read_cache_once();
-  DeviceTable& t = table_for(device_name());
+  DeviceTable& t = current_table();
   {
     std::lock_guard<std::mutex> g(t.mu);
     auto it = t.entries.find(key);
@@ -431,7 +486,7 @@ int tuned_flags(const std::string& key, int lib_flags, cudaStream_t st,
   best.flags &= kScheduleBits | kTensorBits | CIMX_L_TENSOR_ALL_LINES;
   {
     std::lock_guard<std::mutex> g(t.mu);
-    t.entries[key] = best;
+    if (t.entries.insert_or_assign(key, best).second) ++g_entries;
   }
   std::string path;
   {
@@ -473,6 +528,7 @@ int cimx_tune_clear(void) {
     std::lock_guard<std::mutex> gt(dt.second->mu);
     dt.second->entries.clear();
   }
+  g_entries = 0;
   return CIMX_OK;
 }
 
