@@ -320,12 +320,26 @@ int cimx_separable(const CimxArray* in, const CimxArray* out, const CimxPass* pa
     ds[i].out = dst;
     ds[i].tout = out->dtype;
     const int kind = tensor_kind(ds[i]);
-    if (kind == 1)
+    if (kind == 1) {
       rc = launch_tcs_pass(ds[i], st);
-    else if (kind == 2)
+    } else if (kind == 2) {
       rc = launch_tc_pass(ds[i], st);
-    else
-      rc = launch_generic_pass(ds[i], st);
+    } else {
+      // a pass list the fused kernels do not take as a whole (axes out of
+      // ascending order, as the edge filters' edge-then-smooth chains along
+      // axis 1 or 2): each pass on its own still runs on a fast kernel when
+      // one covers it (the stream kernel for a leading axis, the slab for a
+      // pass along the second-to-last axis), the same chain as the generic
+      // kernel. CIMX_L_NO_FUSION keeps the generic kernels.
+      rc = CIMX_FUSED_DECLINED;
+      if (!(lib_flags & CIMX_L_NO_FUSION)) {
+        CimxArray s_arr = i == 0 ? *in : *out, d_arr = *out;
+        s_arr.data = const_cast<void*>(src);
+        d_arr.data = dst;
+        rc = try_fused(&s_arr, &d_arr, &ds[i], 1, lib_flags, st);
+      }
+      if (rc == CIMX_FUSED_DECLINED) rc = launch_generic_pass(ds[i], st);
+    }
     src = dst;
     tsrc = out->dtype;
     dst = (dst == out->data) ? temp : out->data;
