@@ -220,9 +220,9 @@ LAUNCHES_PER_STEP = 6
 # DRAM bytes per launch measured by ncu on a smaller stack: (bytes, slices of
 # that stack, profile file)
 TRAFFIC = {
-    "slab f32->f32 gaussian y,x K=17,17": (201.398272e6 + 162.961920e6, 48,
+    "slab f32->f32 gaussian y,x K=17,17": (201.404672e6 + 162.276608e6, 48,
                                            "k_slab_f32_gaussian_yx_48x1024x1024_and_2048x2048.md"),
-    "volume u16->f32 sobel K=3,3,3": (134.852352e6 + 211.893248e6, 64,
+    "volume u16->f32 sobel K=3,3,3": (135.097344e6 + 212.728064e6, 64,
                                       "k_vol_u16_f32_sobel_64x1024x1024.md"),
 }
 
