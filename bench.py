@@ -656,6 +656,18 @@ def run_tiles(torch, dev, reps=3, check=64, n_tiles=4096):
     cpu_s = time.perf_counter() - t0
     spx = sum(h.shape[0] * h.shape[1] for h in host)
     oracle_ok = all(np.array_equal(b.outputs[i].cpu().numpy(), e) for i, e in zip(sample, exp))
+    # end to end from host memory: the same tiles held on the host through
+    # RegionStream (pinned staging, copies overlapped with the launches),
+    # results back in host memory
+    host_tiles = [t.cpu().numpy() for t in tiles]
+    rs = batch.RegionStream(host_tiles, sigmas)
+    rs.run()
+    t0 = time.perf_counter()
+    res = rs.run()
+    e2e_s = time.perf_counter() - t0
+    e2e_same = all(np.array_equal(res[i], b.outputs[i].cpu().numpy())
+                   for i in range(0, len(tiles), step))
+    del res, host_tiles, rs
     # compute roofline: the useful float32 FMAs of the path per output pixel
     # (K taps of each Gaussian pass, 3 + 3 taps of each sobel direction);
     # the halo the kernel recomputes around every 64 x 64 block is not useful work
@@ -670,6 +682,12 @@ def run_tiles(torch, dev, reps=3, check=64, n_tiles=4096):
             "pixels": npx, "batched_ms": ms_b, "batched_gpx_s": npx / (ms_b * 1e-3) / 1e9,
             "per_tile_ms": ms_t, "per_tile_gpx_s": npx / (ms_t * 1e-3) / 1e9,
             "speedup": ms_t / ms_b, "launches_batched": 1, "launches_per_tile": "about 7 per tile",
+            "e2e_from_host": {"s": e2e_s, "gpx_s": npx / e2e_s / 1e9,
+                              "h2d_bytes": 3 * npx, "d2h_bytes": 4 * npx,
+                              "bit_identical": bool(e2e_same),
+                              "path": "cucim_b200.batch.RegionStream: host tiles gathered into "
+                                      "pinned chunks, copies and launches overlapped, results "
+                                      "copied back into host arrays"},
             "roofline": {"bound": "fp32", "achieved": useful_tflops, "peak": fp32_nominal,
                          "unit": "TFLOP/s", "frac": useful_tflops / fp32_nominal,
                          "note": "useful float32 FMAs (2K + 12 per output pixel) over the nominal "

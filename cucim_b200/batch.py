@@ -14,7 +14,9 @@ within a row (a C-contiguous tile, or a region view of a larger slide: rows
 may be any pitch apart); its output is (H, W) float32 (C-contiguous or a
 region view). `TileBatch.from_regions(slide, regions, sigmas)` builds the
 batch straight from regions of a whole-slide image held on the device, the
-way a slide reader's read_region results feed it, without copying tiles.
+way a slide reader's read_region results feed it, without copying tiles;
+`RegionStream` takes tiles (or slide regions) held in host memory through
+the same launch chunk by chunk, its copies overlapped with the filtering.
 The gaussian uses mode 'nearest' and truncate 4 (the defaults of
 `skimage.filters.gaussian`), the sobel mode 'reflect'; every tile is
 filtered as an image of its own, exactly as the per-tile calls would.
@@ -22,6 +24,7 @@ filtered as an image of its own, exactly as the per-tile calls would.
 
 import ctypes
 import math
+import os
 
 import numpy as np
 
@@ -152,6 +155,154 @@ class TileBatch:
             with torch.cuda.graph(g, stream=s):
                 self.run()
         return g
+
+
+class RegionStream:
+    """Tiles held in host memory through the batched launch, with the copies
+    overlapped: the ingest side of a whole-slide pipeline, where a reader
+    (cuCIM's read_region, a TIFF decoder) leaves tiles in host memory.
+
+        rs = RegionStream(host_tiles, sigmas)          # or .from_regions(host_slide, regions, sigmas)
+        results = rs.run()                             # float32 numpy arrays, input order
+
+    The tiles go in chunks of about `chunk_pixels` pixels through two sets
+    of buffers: while chunk i is filtered, host threads gather chunk i + 1
+    into pinned memory and its copy to the device runs on its own stream,
+    and chunk i - 1's results come back on a third stream; events order the
+    reuse of every buffer. Each chunk is one `TileBatch` launch (tables
+    prepared once, here), so the results are bit-identical to `TileBatch`
+    on the same tiles."""
+
+    def __init__(self, host_tiles, sigmas, chunk_pixels=1 << 26, device=None, truncate=4.0,
+                 threads=None):
+        import torch
+
+        if len(host_tiles) != len(sigmas):
+            raise ValueError("one sigma per tile")
+        self.device = torch.device("cuda") if device is None else torch.device(device)
+        self.host = [np.asarray(t) for t in host_tiles]
+        for t in self.host:
+            if t.dtype != np.uint8 or t.ndim != 3 or t.shape[2] != 3 or 0 in t.shape:
+                raise ValueError("tiles must be non-empty (H, W, 3) uint8 host arrays")
+        self.sigmas = [float(v) for v in sigmas]
+        self.threads = threads or min(16, os.cpu_count() or 1)
+        # chunks of consecutive tiles, each at most chunk_pixels (or one tile)
+        self.chunks, cur, npx = [], [], 0
+        for i, t in enumerate(self.host):
+            n = t.shape[0] * t.shape[1]
+            if cur and npx + n > chunk_pixels:
+                self.chunks.append(cur)
+                cur, npx = [], 0
+            cur.append(i)
+            npx += n
+        if cur:
+            self.chunks.append(cur)
+        cap = max((sum(self.host[i].shape[0] * self.host[i].shape[1] for i in c)
+                   for c in self.chunks), default=1)
+        dev = self.device
+        self._pin_in = [torch.empty(3 * cap, dtype=torch.uint8).pin_memory() for _ in range(2)]
+        self._pin_out = [torch.empty(cap, dtype=torch.float32).pin_memory() for _ in range(2)]
+        self._dev_in = [torch.empty(3 * cap, dtype=torch.uint8, device=dev) for _ in range(2)]
+        self._dev_out = [torch.empty(cap, dtype=torch.float32, device=dev) for _ in range(2)]
+        # per chunk: each tile's pixel offset and its batch over buffer set c % 2
+        self._layout, self._batches = [], []
+        for c, chunk in enumerate(self.chunks):
+            offs, pos = [], 0
+            for i in chunk:
+                offs.append(pos)
+                pos += self.host[i].shape[0] * self.host[i].shape[1]
+            self._layout.append((offs, pos))
+            din, dout = self._dev_in[c % 2], self._dev_out[c % 2]
+            tiles, outs = [], []
+            for i, o in zip(chunk, offs):
+                h, w = self.host[i].shape[:2]
+                tiles.append(din.narrow(0, 3 * o, 3 * h * w).view(h, w, 3))
+                outs.append(dout.narrow(0, o, h * w).view(h, w))
+            self._batches.append(TileBatch(tiles, [self.sigmas[i] for i in chunk], outputs=outs,
+                                           truncate=truncate))
+        self.npixels = sum(t.shape[0] * t.shape[1] for t in self.host)
+
+    @classmethod
+    def from_regions(cls, slide, regions, sigmas, **kw):
+        """Regions (y, x, height, width) of one (H, W, 3) uint8 slide in host
+        memory (views: a region is read once, by the gather of its chunk)."""
+        s = np.asarray(slide)
+        if s.ndim != 3 or s.shape[2] != 3 or s.dtype != np.uint8:
+            raise ValueError("the slide must be an (H, W, 3) uint8 array")
+        H, W = s.shape[:2]
+        tiles = []
+        for (y, x, h, w) in regions:
+            if not (0 <= y and 0 <= x and h >= 1 and w >= 1 and y + h <= H and x + w <= W):
+                raise ValueError(f"region {(y, x, h, w)} is outside the {H} x {W} slide")
+            tiles.append(s[y:y + h, x:x + w])
+        return cls(tiles, sigmas, **kw)
+
+    def _gather(self, pool, c):
+        """Chunk c's tiles into pinned buffer set c % 2 (host threads)."""
+        offs, n = self._layout[c]
+        buf = self._pin_in[c % 2].numpy()
+
+        def one(k):
+            t = self.host[self.chunks[c][k]]
+            h, w = t.shape[:2]
+            buf[3 * offs[k]:3 * (offs[k] + h * w)].reshape(h, w, 3)[...] = t
+        list(pool.map(one, range(len(self.chunks[c]))))
+        return n
+
+    def _collect(self, pool, c, results):
+        """Chunk c's results out of pinned buffer set c % 2 (after its copy),
+        by host threads."""
+        offs, _ = self._layout[c]
+        buf = self._pin_out[c % 2].numpy()
+
+        def one(k):
+            i = self.chunks[c][k]
+            h, w = self.host[i].shape[:2]
+            results[i] = buf[offs[k]:offs[k] + h * w].reshape(h, w).copy()
+        list(pool.map(one, range(len(self.chunks[c]))))
+
+    def run(self):
+        import concurrent.futures as cf
+
+        import torch
+
+        dev = self.device
+        cs, ks, ds = (torch.cuda.Stream(dev) for _ in range(3))
+        ev_h2d, ev_kernel, ev_d2h = [None, None], [None, None], [None, None]
+        pending = [None, None]  # chunk whose results sit in (or are coming to) pinned set s
+        results = [None] * len(self.host)
+        with cf.ThreadPoolExecutor(self.threads) as pool:
+            for c in range(len(self.chunks)):
+                s = c % 2
+                if ev_h2d[s] is not None:
+                    ev_h2d[s].synchronize()  # pinned input set s is read by its copy
+                n = self._gather(pool, c)
+                with torch.cuda.stream(cs):
+                    if ev_kernel[s] is not None:
+                        cs.wait_event(ev_kernel[s])  # device input set s is read by its kernel
+                    self._dev_in[s][:3 * n].copy_(self._pin_in[s][:3 * n], non_blocking=True)
+                    ev_h2d[s] = torch.cuda.Event()
+                    ev_h2d[s].record(cs)
+                ks.wait_event(ev_h2d[s])
+                if ev_d2h[s] is not None:
+                    ks.wait_event(ev_d2h[s])  # device output set s is read by its copy back
+                self._batches[c].run(stream=ks.cuda_stream)
+                ev_kernel[s] = torch.cuda.Event()
+                ev_kernel[s].record(ks)
+                if pending[s] is not None:
+                    ev_d2h[s].synchronize()  # pinned output set s: take the previous results
+                    self._collect(pool, pending[s], results)
+                with torch.cuda.stream(ds):
+                    ds.wait_event(ev_kernel[s])
+                    self._pin_out[s][:n].copy_(self._dev_out[s][:n], non_blocking=True)
+                    ev_d2h[s] = torch.cuda.Event()
+                    ev_d2h[s].record(ds)
+                pending[s] = c
+            for s in range(2):
+                if pending[s] is not None:
+                    ev_d2h[s].synchronize()
+                    self._collect(pool, pending[s], results)
+        return results
 
 
 def gray_gauss_sobel_per_tile(rgb_tiles, sigmas, outputs=None):

@@ -108,3 +108,40 @@ def test_batch_from_slide_regions(cuda):
     assert bool((out_slide[untouched] == -1.0).all())
     with pytest.raises(ValueError):
         batch.TileBatch.from_regions(slide, [(690, 0, 20, 20)], [1.0])
+
+
+def test_region_stream_from_host_slide(cuda):
+    """Regions of a slide in host memory through RegionStream, in chunks small
+    enough that both buffer sets are reused several times: bit-identical to
+    TileBatch on the same slide held on the device, again on a second run,
+    and to the oracle on a few regions."""
+    from cucim_b200 import batch
+    from oracle import restate as R
+
+    rng = np.random.default_rng(11)
+    slide = rng.integers(0, 256, (700, 900, 3), dtype=np.uint8)
+    regions = [(int(rng.integers(0, 600)), int(rng.integers(0, 800)), int(rng.integers(1, 100)),
+                int(rng.integers(1, 100))) for _ in range(40)] + [(0, 0, 700, 900), (3, 5, 1, 1)]
+    sigmas = [float(v) for v in rng.uniform(0.5, 6.0, len(regions))]
+    rs = batch.RegionStream.from_regions(slide, regions, sigmas, chunk_pixels=60_000)
+    assert len(rs.chunks) > 3
+    got = rs.run()
+    ref = batch.TileBatch.from_regions(torch.as_tensor(slide).cuda(), regions, sigmas).run()
+    assert len(got) == len(regions)
+    for g, r in zip(got, ref):
+        assert g.dtype == np.float32 and np.array_equal(g, r.cpu().numpy())
+    again = rs.run()
+    assert all(np.array_equal(a, b) for a, b in zip(got, again))
+    for k in (0, 7, len(regions) - 2, len(regions) - 1):
+        y, x, h, w = regions[k]
+        exp = R.sk_sobel(R.sk_gaussian(R.rgb2gray(slide[y:y + h, x:x + w]), sigmas[k]))
+        assert np.array_equal(got[k], exp), k
+
+
+def test_region_stream_rejects_bad_input(cuda):
+    from cucim_b200 import batch
+
+    with pytest.raises(ValueError):
+        batch.RegionStream([np.zeros((4, 4, 3), np.float32)], [1.0])
+    with pytest.raises(ValueError):
+        batch.RegionStream.from_regions(np.zeros((10, 10, 3), np.uint8), [(5, 5, 6, 2)], [1.0])
