@@ -308,7 +308,9 @@ __host__ __device__ constexpr int pad8(int c) { return c + (c >> 3); }
 //   mbarrier | y taps, x taps as (t, t) pairs |
 //   float input: raw x 2 (BY x BX floats each; the next slab's tile loads
 //                while this one is computed) | s_mid (TY/2 row pairs x RXQ float2)
-//   other input: s_in (RY x RXS floats) | union { raw (T), s_mid }
+//   other input: s_in (RY x RXS floats) | s_mid | raw (T; loads while the
+//                passes run) for taps buckets up to 48, else
+//                s_in | union { raw (T), s_mid }
 template <class T, int KB>
 struct Geom {
   static constexpr bool F32 = sizeof(T) == 4;
@@ -331,8 +333,6 @@ struct Geom {
   static constexpr int OFF_A = OFF_W + 2 * KB * 8;  // raw (f32) or s_in
   static constexpr int SZ_A = F32 ? NBUF * RAWP : RY * RXS * 4;
   static constexpr int OFF_B = (OFF_A + SZ_A + 127) / 128 * 128;  // s_mid (f32) or union
-  static constexpr int SZ_B = F32 ? MID : (RAW > MID ? RAW : MID);
-  static constexpr int SMEM = OFF_B + SZ_B;
   // threads: enough for every y-pass item (NPAIR column pairs x TY/P row
   // groups) in one round; the x pass has TY/2 x TX/P = 256 items
   static constexpr int NT = ((NPAIR * (kSlabTY / P) + 31) / 32) * 32;
@@ -341,6 +341,16 @@ struct Geom {
   // three up to 320 threads (64 registers), two beyond (three would leave
   // 56 registers and spill)
   static constexpr int MINB = NT <= 320 ? 3 : 2;
+  // other inputs: the raw tile gets a buffer of its own (after s_mid) where
+  // that keeps MINB CTAs per SM by shared memory (taps buckets up to 48), so
+  // that the next slab's tile loads while this one is computed; else it
+  // shares its buffer with s_mid
+  static constexpr int SMEM_U = OFF_B + (RAW > MID ? RAW : MID);
+  static constexpr int OFF_R = (OFF_B + MID + 127) / 128 * 128;
+  static constexpr int SMEM_S = OFF_R + RAWP;
+  static constexpr int fit(int s) { return (228 * 1024) / (s + 1024); }
+  static constexpr bool SEP = !F32 && fit(SMEM_S) >= (fit(SMEM_U) < MINB ? fit(SMEM_U) : MINB);
+  static constexpr int SMEM = F32 ? OFF_B + MID : (SEP ? SMEM_S : SMEM_U);
 };
 
 __device__ __forceinline__ long long floor_div(long long a, long long b) {
@@ -468,7 +478,7 @@ __global__ void __launch_bounds__(Geom<T, KB>::NT, Geom<T, KB>::MINB) k_slab(con
   uint64_t* bar = reinterpret_cast<uint64_t*>(smem);  // bar[0], bar[1]: one per raw buffer
   f2* wy = reinterpret_cast<f2*>(smem + G::OFF_W);
   f2* wx = wy + KB;
-  T* raw0 = reinterpret_cast<T*>(smem + (G::F32 ? G::OFF_A : G::OFF_B));
+  T* raw0 = reinterpret_cast<T*>(smem + (G::F32 ? G::OFF_A : (G::SEP ? G::OFF_R : G::OFF_B)));
   float* s_in = reinterpret_cast<float*>(smem + G::OFF_A);  // non-float inputs only
   f2* s_mid = reinterpret_cast<f2*>(smem + G::OFF_B);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -498,8 +508,6 @@ __global__ void __launch_bounds__(Geom<T, KB>::NT, Geom<T, KB>::MINB) k_slab(con
   const long long ys = y0 - ay, xst = x0 - ax;
   const long long xs = floor_div(xst, G::VE) * G::VE;  // 16-byte aligned TMA start column
   const int off = static_cast<int>(xst - xs);
-  // float input: pairs are read from the TMA tile starting at column off - sh
-  const int sh = (TMA && G::F32) ? (off & 1) : 0;
   // staged columns [cl, cr) and rows [rl, rr) lie inside the array
   auto clampi = [](long long v, long long lo, long long hi) {
     return static_cast<int>(v < lo ? lo : (v > hi ? hi : v));
@@ -508,6 +516,14 @@ __global__ void __launch_bounds__(Geom<T, KB>::NT, Geom<T, KB>::MINB) k_slab(con
   const int cr = clampi(a.X - xst, cl, G::RX);
   const int rl = clampi(-ys, 0, G::RY);
   const int rr = clampi(a.Y - ys, rl, G::RY);
+  // other inputs with a raw buffer of their own: a tile whose staged region
+  // lies inside the array skips the conversion to s_in, the y pass reads
+  // element pairs of the raw tile (the same for every thread of the CTA)
+  const bool direct = !G::F32 && G::SEP && TMA && rl == 0 && rr == G::RY && cl == 0 &&
+                      cr == G::RX;
+  // float input, or a direct tile: pairs are read from the TMA tile starting
+  // at column off - sh (an even column)
+  const int sh = ((TMA && G::F32) || direct) ? (off & 1) : 0;
   // float input: two TMA buffers; the copy for the next slab is issued before
   // the current slab is computed. Other inputs: one buffer.
   constexpr int NBUF = G::NBUF;
@@ -519,8 +535,10 @@ __global__ void __launch_bounds__(Geom<T, KB>::NT, Geom<T, KB>::MINB) k_slab(con
   };
   // float input, one buffer: the y pass is the last reader of the raw tile
   // (the x pass reads s_mid), so the next slab's tile is issued right after
-  // it and lands while the x pass runs
-  constexpr bool kEarly = G::F32 && NBUF == 1;
+  // it and lands while the x pass runs. The same holds for other inputs with
+  // a raw buffer of their own (the conversion to s_in, or on a direct tile
+  // the y pass, is the last reader).
+  constexpr bool kEarly = (G::F32 || G::SEP) && NBUF == 1;
   if (TMA && (NBUF == 2 || kEarly) && threadIdx.x == 0 && blockIdx.z < a.B) issue(blockIdx.z, 0);
   long long it = 0;
   for (long long b = blockIdx.z; b < a.B; b += gridDim.z, ++it) {
@@ -595,7 +613,7 @@ __global__ void __launch_bounds__(Geom<T, KB>::NT, Geom<T, KB>::MINB) k_slab(con
         row[c] = v;
       }
     }
-  } else {
+  } else if (!direct) {
     // convert to float into the staging buffer at column c (pairs aligned)
     float* dst = G::F32 ? reinterpret_cast<float*>(raw) : s_in;
     const int stride = G::F32 ? G::BX : G::RXS;
@@ -627,9 +645,25 @@ __global__ void __launch_bounds__(Geom<T, KB>::NT, Geom<T, KB>::MINB) k_slab(con
       f2 acc[P];
 #pragma unroll
       for (int p = 0; p < P; ++p) acc[p] = 0ull;
-      const f2* col = reinterpret_cast<const f2*>(src + rg * stride + soff + e);
-      chain2(acc, wy, a.py.K, a.py.skip,
-             [&](int qb, int j) { return col[(qb + j) * (stride / 2)]; });
+      if constexpr (!G::F32 && G::SEP && TMA) {
+        if (direct) {
+          // the pair (e - sh, e - sh + 1) of staged columns, one aligned
+          // 2-element load from the raw tile, widened exactly
+          using Pair = typename std::conditional<sizeof(T) == 2, uint32_t, uint16_t>::type;
+          constexpr int kBits = 8 * static_cast<int>(sizeof(T));
+          const Pair* colr = reinterpret_cast<const Pair*>(raw + rg * G::BX + off - sh + e);
+          chain2(acc, wy, a.py.K, a.py.skip, [&](int qb, int j) {
+            const uint32_t w = colr[(qb + j) * (G::BX / 2)];
+            return pack2(exact_float<T>(static_cast<T>(w & ((1u << kBits) - 1))),
+                         exact_float<T>(static_cast<T>(w >> kBits)));
+          });
+        }
+      }
+      if (!direct) {
+        const f2* col = reinterpret_cast<const f2*>(src + rg * stride + soff + e);
+        chain2(acc, wy, a.py.K, a.py.skip,
+               [&](int qb, int j) { return col[(qb + j) * (stride / 2)]; });
+      }
       const long long gx = xst + e - sh;
       if (a.has_x) {
         const bool f0 = mx == CIMX_MODE_CONSTANT && (gx < 0 || gx >= a.X);
@@ -701,10 +735,11 @@ __global__ void __launch_bounds__(Geom<T, KB>::NT, Geom<T, KB>::MINB) k_slab(con
       }
     }
   }
-  // shared buffers are reused by the next slab. With float input, TMA and an
-  // x pass the barrier after the next slab's tile wait already orders this
-  // slab's x pass (the last reader of s_mid) before the next y pass, and the
-  // raw tile is not shared with s_mid: no barrier here
+  // shared buffers are reused by the next slab. With a raw buffer of its own
+  // (float input, or SEP), TMA and an x pass, the barrier after the next
+  // slab's tile wait already orders this slab's x pass (the last reader of
+  // s_mid) before the next y pass, and this slab's y pass (the last reader of
+  // s_in) before the next conversion: no barrier here
   if (!(TMA && kEarly && a.has_x)) __syncthreads();
   if (TMA && kEarly && !a.has_x && threadIdx.x == 0 && b + gridDim.z < a.B)
     issue(b + gridDim.z, 0);
@@ -733,16 +768,17 @@ int launch_slab_kb(SlabArgs& a, cudaStream_t st) {
   if (a.tiles_y > 65535) return CIMX_FUSED_DECLINED;
   // enough CTAs to fill the GPU several times over; each walks a stride of
   // slabs so that it can load the next slab's tile while computing the
-  // current one (float input: about four slabs per CTA, at least ~12 CTAs
-  // per SM)
+  // current one (float input, or other inputs with a raw buffer of their
+  // own: about four slabs per CTA, at least ~12 CTAs per SM)
   const long long per_slab = a.tiles_x * a.tiles_y;
+  constexpr bool kWalk = G::F32 || G::SEP;
   long long zs;
   if (G::NBUF == 2)
     zs = std::max<long long>(
         1, std::min<long long>({a.B, 65535LL, (148LL * 8 + per_slab - 1) / per_slab}));
-  else if (G::F32 && tma && a.span > 0)  // a tuned or forced span (any span is exact)
+  else if (kWalk && tma && a.span > 0)  // a tuned or forced span (any span is exact)
     zs = std::max<long long>(1, std::min<long long>({a.B, 65535LL, (a.B + a.span - 1) / a.span}));
-  else if (G::F32 && tma)
+  else if (kWalk && tma)
     zs = std::max<long long>(1, std::min<long long>({a.B, 65535LL,
                                                      std::max<long long>((a.B + 3) / 4,
                                                      (148LL * 12 + per_slab - 1) / per_slab)}));

@@ -181,9 +181,17 @@ int try_fused(const CimxArray* in, const CimxArray* out, PassDesc* ds, int npass
     }
   }
   const int tail_in = lead.empty() ? in->dtype : D;
+  // a lone pass along the last axis over float32 data runs on the slab
+  // kernel behind an identity y pass (one tap of 1: fma(v, 1, +0) = v, kept
+  // as float32, exact). A -0 input becomes +0, which the x pass's chain from
+  // +0 cannot tell apart. Measured on 16 x 2048 x 2048 with 9 taps: 148 us
+  // against 266 us on the generic row kernel. For 8- and 16-bit input the
+  // generic row kernel is the faster (uint16: 240 us against 316 us).
+  const bool y_identity = !tail.empty() && nd >= 2 && ds[tail[0]].axis == nd - 1 &&
+                          tail_in == DT_F32 && D == DT_F32;
   if (!tail.empty()) {
     // the slab kernel needs a pass along the second-to-last axis
-    if (nd < 2 || ds[tail[0]].axis != nd - 2) return CIMX_FUSED_DECLINED;
+    if (nd < 2 || (ds[tail[0]].axis != nd - 2 && !y_identity)) return CIMX_FUSED_DECLINED;
     if (!fast_pair(tail_in, D)) return CIMX_FUSED_DECLINED;
     for (int i : tail)
       if (!trim(ds[i], kSlabMaxK, tr[i])) return CIMX_FUSED_DECLINED;
@@ -234,6 +242,15 @@ int try_fused(const CimxArray* in, const CimxArray* out, PassDesc* ds, int npass
     a.Y = nd >= 2 ? in->shape[nd - 2] : 1;
     a.B = (a.X * a.Y == 0) ? 0 : n / (a.X * a.Y);
     int pass_in = tsrc;
+    if (y_identity) {
+      a.py = SlabPass{};
+      a.py.K = 1;
+      a.py.K8 = 8;
+      a.py.mode = CIMX_MODE_NEAREST;  // no halo: K = 1, anchor 0
+      a.py.dt = pass_in;
+      a.py.w[0] = 1.f;
+      a.has_y = 1;
+    }
     for (int i : tail) {
       const bool is_x = ds[i].axis == nd - 1;
       fill_slab_pass(is_x ? a.px : a.py, ds[i], tr[i], pass_in);

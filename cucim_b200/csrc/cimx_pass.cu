@@ -99,11 +99,58 @@ __device__ __forceinline__ float staged_f32(const float* line, long long stride,
   return m < 0 ? cv : __ldg(line + m * stride);
 }
 
+// Element m of a line as W: typed for the common input dtypes (TI = the
+// element type), by the runtime dtype code otherwise (TI = void).
+template <class TI, class W>
+__device__ __forceinline__ W line_value(const void* line, long long m, int dt) {
+  if constexpr (std::is_void<TI>::value) return load_as<W>(line, m, dt);
+  else return to_w<W>(static_cast<const TI*>(line)[m]);
+}
+
+// Stage columns c0 .. c0 + n - 1 of one line into the padded row buffer as
+// W. The in-range columns load straight from the line, eight loads in flight
+// per thread before the shared stores; the few beyond either end (at most
+// the halo) go through the boundary map in a loop of their own, the fill
+// value where it gives -1.
+template <class TI, class W>
+__device__ __forceinline__ void stage_row(W* rb, const void* line, int dt, long long c0, int n,
+                                          long long L, int mode, W cv, int lane, int nl) {
+  const long long lo = -c0, hi = L - c0;
+  const int jlo = static_cast<int>(lo < 0 ? 0 : (lo > n ? n : lo));
+  const int jhi = static_cast<int>(hi < jlo ? jlo : (hi > n ? n : hi));
+  const void* base = static_cast<const unsigned char*>(line) +
+                     c0 * static_cast<long long>(dtype_size(dt));  // column c0
+  for (int jb = jlo + lane; jb < jhi; jb += 8 * nl) {
+    W v[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int j = jb + q * nl;
+      if (j < jhi) v[q] = line_value<TI, W>(base, j, dt);
+    }
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int j = jb + q * nl;
+      if (j < jhi) rb[j + (j >> 3)] = v[q];
+    }
+  }
+  const int nout = jlo + (n - jhi);
+  for (int t = lane; t < nout; t += nl) {
+    const int j = t < jlo ? t : jhi + (t - jlo);
+    const long long m = map_coord_near(c0 + j, L, mode);
+    rb[j + (j >> 3)] = m < 0 ? cv : line_value<TI, W>(line, m, dt);
+  }
+}
+
 // Filter along the contiguous last axis (inner == 1). Block = (seg_threads,
 // rows); each row buffer is padded by one word every 8 so that lanes reading
-// at a stride of P words hit distinct banks.
-template <class W, bool SKIPZ>
-__global__ void __launch_bounds__(256) k_rows(GArgs a, TapBlock<W> tb) {
+// at a stride of P words hit distinct banks. For 32- and 64-bit outputs the
+// P outputs of a thread go back through the row buffer, so that the stores
+// of a warp cover consecutive elements. TI: the input element type, or void
+// for the runtime-typed loads. Six CTAs per SM with float weights (40
+// registers, a few spilled), four with double: measured faster than the
+// compiler's own choice (48-64 registers) on every dtype pair.
+template <class W, bool SKIPZ, class TI>
+__global__ void __launch_bounds__(256, sizeof(W) == 4 ? 6 : 4) k_rows(GArgs a, TapBlock<W> tb) {
   extern __shared__ __align__(16) unsigned char sm_raw[];
   W* taps = reinterpret_cast<W*>(sm_raw);
   const int nthr = blockDim.x * blockDim.y;
@@ -113,10 +160,6 @@ __global__ void __launch_bounds__(256) k_rows(GArgs a, TapBlock<W> tb) {
   const int span = seg + a.K8 + P;
   const int pspan = span + (span >> 3) + 1;
   W* rb = taps + a.K8 + threadIdx.y * pspan;
-  // mapped line coordinate of each staged column (-1: the fill value), shared
-  // by the rows of the CTA: the boundary map runs once per column
-  long long* colmap = reinterpret_cast<long long*>(
-      sm_raw + ((sizeof(W) * ((size_t)a.K8 + (size_t)blockDim.y * pspan) + 7) & ~(size_t)7));
 
   const long long sg = blockIdx.x % a.tiles_b;
   const long long rg = blockIdx.x / a.tiles_b;
@@ -124,70 +167,48 @@ __global__ void __launch_bounds__(256) k_rows(GArgs a, TapBlock<W> tb) {
   const long long x0 = sg * seg;
   const W cv = fill_value<W>(a.cval, a.cval_as_input, a.tin);
   const long long rbase = row * a.L;
-  const bool interior = x0 - a.anchor >= 0 && x0 - a.anchor + span <= a.L;
-  const bool walk = sizeof(W) == 4 && a.tin == DT_F32 && interior;
-  if (!walk) {  // the same for every thread of the CTA
-    for (int j = tid; j < span; j += nthr) colmap[j] = map_coord_near(x0 - a.anchor + j, a.L, a.mode);
-    __syncthreads();
-  }
-  if (row < a.outer) {
-    if (walk) {
-      // float32 input, span inside the row: plain loads, eight in flight
-      const float* line = static_cast<const float*>(a.in) + rbase + (x0 - a.anchor);
-      for (int jb = threadIdx.x; jb < span; jb += 8 * blockDim.x) {
-        float v[8];
-#pragma unroll
-        for (int q = 0; q < 8; ++q) {
-          const int j = jb + q * blockDim.x;
-          v[q] = j < span ? __ldg(line + j) : 0.f;
-        }
-#pragma unroll
-        for (int q = 0; q < 8; ++q) {
-          const int j = jb + q * blockDim.x;
-          if (j < span) rb[j + (j >> 3)] = v[q];
-        }
-      }
-    } else if (sizeof(W) == 4 && a.tin == DT_F32) {
-      // float32 input: eight loads in flight per thread before the stores
-      const float* line = static_cast<const float*>(a.in) + rbase;
-      for (int jb = threadIdx.x; jb < span; jb += 8 * blockDim.x) {
-        float v[8];
-#pragma unroll
-        for (int q = 0; q < 8; ++q) {
-          const int j = jb + q * blockDim.x;
-          v[q] = 0.f;
-          if (j < span) {
-            const long long m = colmap[j];
-            v[q] = m < 0 ? (float)cv : __ldg(line + m);
-          }
-        }
-#pragma unroll
-        for (int q = 0; q < 8; ++q) {
-          const int j = jb + q * blockDim.x;
-          if (j < span) rb[j + (j >> 3)] = v[q];
-        }
-      }
-    } else {
-      for (int j = threadIdx.x; j < span; j += blockDim.x) {
-        const long long m = colmap[j];
-        rb[j + (j >> 3)] = m < 0 ? cv : load_as<W>(a.in, rbase + m, a.tin);
-      }
-    }
+  const bool live = row < a.outer;
+  if (live) {
+    // only the columns that the stored outputs (x < L) read: a row shorter
+    // than the segment stages L - x0 + K8 + P columns, not the whole span
+    const long long need = a.L - x0 + a.K8 + P;
+    const int n = need < span ? static_cast<int>(need) : span;
+    const void* line = static_cast<const unsigned char*>(a.in) +
+                       rbase * static_cast<long long>(dtype_size(a.tin));
+    stage_row<TI, W>(rb, line, a.tin, x0 - a.anchor, n, a.L, a.mode, cv, threadIdx.x,
+                     blockDim.x);
   }
   __syncthreads();
-  if (row >= a.outer) return;
   const int b = threadIdx.x * P;
   W acc[P];
 #pragma unroll
   for (int p = 0; p < P; ++p) acc[p] = W(0);
-  tap_loop<W, SKIPZ>(acc, taps, a.K, [&](int q) {
-    const int x = b + q;
-    return rb[x + (x >> 3)];
-  });
+  if (live)
+    tap_loop<W, SKIPZ>(acc, taps, a.K, [&](int q) {
+      const int x = b + q;
+      return rb[x + (x >> 3)];
+    });
+  if (dtype_size(a.tout) < 4) {
+    // 8- and 16-bit outputs: straight from the accumulators (measured faster
+    // than going back through the buffer)
+    if (!live) return;
 #pragma unroll
-  for (int p = 0; p < P; ++p) {
-    const long long x = x0 + b + p;
-    if (x < a.L) store_cast<W>(a.out, rbase + x, acc[p], a.tout);
+    for (int p = 0; p < P; ++p) {
+      const long long x = x0 + b + p;
+      if (x < a.L) store_cast<W>(a.out, rbase + x, acc[p], a.tout);
+    }
+    return;
+  }
+  __syncthreads();  // every window read is done before the outputs overwrite the buffer
+  if (live) {
+#pragma unroll
+    for (int p = 0; p < P; ++p) rb[b + p + ((b + p) >> 3)] = acc[p];
+  }
+  __syncthreads();  // a row spans blockDim.x / 32 warps
+  if (!live) return;
+  for (int j = threadIdx.x; j < seg; j += blockDim.x) {
+    const long long x = x0 + j;
+    if (x < a.L) store_cast<W>(a.out, rbase + x, rb[j + (j >> 3)], a.tout);
   }
 }
 
@@ -451,7 +472,7 @@ __global__ void __launch_bounds__(256) k_direct(GArgs a) {
 }
 
 // Row kernel geometry for lines of L samples: threads per segment, rows per
-// CTA and the dynamic shared memory (taps, padded row buffers, column map).
+// CTA and the dynamic shared memory (taps, padded row buffers).
 struct RowGeom {
   int seg_threads, ry, seg;
   size_t smem;
@@ -464,7 +485,7 @@ inline RowGeom row_geom(long long L, int K8, size_t wsize) {
   g.seg = g.seg_threads * P;
   const int span = g.seg + K8 + P;
   const int pspan = span + (span >> 3) + 1;
-  g.smem = ((wsize * ((size_t)K8 + (size_t)g.ry * pspan) + 7) & ~(size_t)7) + 8 * (size_t)span;
+  g.smem = wsize * ((size_t)K8 + (size_t)g.ry * pspan);
   return g;
 }
 
@@ -473,11 +494,42 @@ void allow_big_smem(Kern k) {
   cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem);
 }
 
+// k_rows with typed loads for the input dtypes the fast kernels also take
+// (and float64 with double weights), runtime-typed loads for the rest
+template <class W, bool SKIPZ>
+void launch_rows(const GArgs& a, const TapBlock<W>& tb, dim3 grid, dim3 block, size_t smem,
+                 cudaStream_t st) {
+  static std::once_flag once;
+  std::call_once(once, [] {
+    allow_big_smem(k_rows<W, SKIPZ, void>);
+    if constexpr (std::is_same<W, float>::value) {
+      allow_big_smem(k_rows<W, SKIPZ, float>);
+      allow_big_smem(k_rows<W, SKIPZ, uint16_t>);
+      allow_big_smem(k_rows<W, SKIPZ, uint8_t>);
+    } else {
+      allow_big_smem(k_rows<W, SKIPZ, double>);
+    }
+  });
+  if constexpr (std::is_same<W, float>::value) {
+    switch (a.tin) {
+      case DT_F32: k_rows<W, SKIPZ, float><<<grid, block, smem, st>>>(a, tb); return;
+      case DT_U16: k_rows<W, SKIPZ, uint16_t><<<grid, block, smem, st>>>(a, tb); return;
+      case DT_U8: k_rows<W, SKIPZ, uint8_t><<<grid, block, smem, st>>>(a, tb); return;
+      default: break;
+    }
+  } else {
+    if (a.tin == DT_F64) {
+      k_rows<W, SKIPZ, double><<<grid, block, smem, st>>>(a, tb);
+      return;
+    }
+  }
+  k_rows<W, SKIPZ, void><<<grid, block, smem, st>>>(a, tb);
+}
+
 template <class W, bool SKIPZ>
 int launch_t(GArgs a, const TapBlock<W>& tb, bool direct, cudaStream_t st) {
   static std::once_flag once;
   std::call_once(once, [] {
-    allow_big_smem(k_rows<W, SKIPZ>);
     allow_big_smem(k_cols<W, SKIPZ>);
     if constexpr (std::is_same<W, float>::value) allow_big_smem(k_cols_pairs<SKIPZ>);
   });
@@ -490,7 +542,7 @@ int launch_t(GArgs a, const TapBlock<W>& tb, bool direct, cudaStream_t st) {
     const RowGeom g = row_geom(a.L, a.K8, sizeof(W));
     a.tiles_b = (a.L + g.seg - 1) / g.seg;
     const long long blocks = ((a.outer + g.ry - 1) / g.ry) * a.tiles_b;
-    k_rows<W, SKIPZ><<<(unsigned)blocks, dim3(g.seg_threads, g.ry), g.smem, st>>>(a, tb);
+    launch_rows<W, SKIPZ>(a, tb, dim3((unsigned)blocks), dim3(g.seg_threads, g.ry), g.smem, st);
   } else {
     if constexpr (std::is_same<W, float>::value) {
       // float32 input along lines longer than one k_cols tile: column pairs
