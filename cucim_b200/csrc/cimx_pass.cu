@@ -100,7 +100,9 @@ __device__ __forceinline__ float staged_f32(const float* line, long long stride,
 }
 
 // Element m of a line as W: typed for the common input dtypes (TI = the
-// element type), by the runtime dtype code otherwise (TI = void).
+// element type), by the runtime dtype code otherwise (TI = void). Plain
+// loads: the read-only data cache path measured no faster on columns and
+// slower on short rows (20000 x 100 float32: 28.5 -> 42.3 us).
 template <class TI, class W>
 __device__ __forceinline__ W line_value(const void* line, long long m, int dt) {
   if constexpr (std::is_void<TI>::value) return load_as<W>(line, m, dt);
@@ -213,9 +215,12 @@ __global__ void __launch_bounds__(256, sizeof(W) == 4 ? 6 : 4) k_rows(GArgs a, T
 }
 
 // Filter along a strided axis (inner > 1). Block = (32 inner columns, 8);
-// each thread produces P consecutive outputs of one column.
-template <class W, bool SKIPZ>
-__global__ void __launch_bounds__(256) k_cols(GArgs a, TapBlock<W> tb) {
+// each thread produces P consecutive outputs of one column. With typed loads
+// (TI: float32 input with float weights, float64 with double weights; void:
+// runtime-typed) a tile inside the line walks its rows directly; otherwise
+// each staged row's mapped offset comes from a table built once per CTA.
+template <class W, bool SKIPZ, class TI>
+__global__ void __launch_bounds__(256, sizeof(W) == 4 ? 6 : 4) k_cols(GArgs a, TapBlock<W> tb) {
   extern __shared__ __align__(16) unsigned char sm_raw[];
   W* taps = reinterpret_cast<W*>(sm_raw);
   const int tid = threadIdx.y * kColTI + threadIdx.x;
@@ -236,7 +241,12 @@ __global__ void __launch_bounds__(256) k_cols(GArgs a, TapBlock<W> tb) {
   const W cv = fill_value<W>(a.cval, a.cval_as_input, a.tin);
   const long long obase = o * a.L;
   const bool interior = l0 - a.anchor >= 0 && l0 - a.anchor + span <= a.L;
-  const bool walk = sizeof(W) == 4 && a.tin == DT_F32 && interior;
+  // typed loads (float32 input with float weights, float64 with double):
+  // an interior tile walks its rows, eight loads in flight; the other
+  // dtypes take one runtime-typed load per row (measured: eight-wide
+  // staging of those made them 5-8 % slower, float64 1.6x faster)
+  constexpr bool kTyped = !std::is_void<TI>::value;
+  const bool walk = interior && kTyped;
   if (!walk) {  // the same for every thread of the CTA
     for (int j = tid; j < span; j += kColTI * kColTY) {
       const long long cj = l0 - a.anchor + j;
@@ -245,35 +255,19 @@ __global__ void __launch_bounds__(256) k_cols(GArgs a, TapBlock<W> tb) {
     }
     __syncthreads();
   }
-  if (walk) {
-    // float32 input, span inside the line: a pointer walk, eight loads in flight
-    const long long stride = a.inner;
-    const float* col = static_cast<const float*>(a.in) + (obase + l0 - a.anchor) * stride + i;
+  if constexpr (kTyped) {
+    // element offset of staged row j (column 0): a walk inside the line,
+    // the table otherwise (-1: the fill value); eight loads in flight
+    const long long walk0 = (obase + l0 - a.anchor) * a.inner;
     for (int jb = threadIdx.y; jb < span; jb += 8 * kColTY) {
-      float v[8];
+      W v[8];
 #pragma unroll
       for (int q = 0; q < 8; ++q) {
         const int j = jb + q * kColTY;
-        v[q] = (j < span && i < a.inner) ? __ldg(col + (long long)j * stride) : 0.f;
-      }
-#pragma unroll
-      for (int q = 0; q < 8; ++q) {
-        const int j = jb + q * kColTY;
-        if (j < span) buf[j * kColTI + threadIdx.x] = v[q];
-      }
-    }
-  } else if (sizeof(W) == 4 && a.tin == DT_F32) {
-    // float32 input: eight loads in flight per thread before the stores
-    const float* col = static_cast<const float*>(a.in) + i;
-    for (int jb = threadIdx.y; jb < span; jb += 8 * kColTY) {
-      float v[8];
-#pragma unroll
-      for (int q = 0; q < 8; ++q) {
-        const int j = jb + q * kColTY;
-        v[q] = 0.f;
+        v[q] = W(0);
         if (j < span && i < a.inner) {
-          const long long off = rowoff[j];
-          v[q] = off < 0 ? (float)cv : __ldg(col + off);
+          const long long off = walk ? walk0 + (long long)j * a.inner : rowoff[j];
+          v[q] = off < 0 ? cv : line_value<TI, W>(a.in, off + i, a.tin);
         }
       }
 #pragma unroll
@@ -494,6 +488,30 @@ void allow_big_smem(Kern k) {
   cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem);
 }
 
+// k_cols with typed loads for float32 (float weights) and float64 input
+template <class W, bool SKIPZ>
+void launch_cols(const GArgs& a, const TapBlock<W>& tb, dim3 grid, dim3 block, size_t smem,
+                 cudaStream_t st) {
+  static std::once_flag once;
+  std::call_once(once, [] {
+    allow_big_smem(k_cols<W, SKIPZ, void>);
+    if constexpr (std::is_same<W, float>::value) allow_big_smem(k_cols<W, SKIPZ, float>);
+    else allow_big_smem(k_cols<W, SKIPZ, double>);
+  });
+  if constexpr (std::is_same<W, float>::value) {
+    if (a.tin == DT_F32) {
+      k_cols<W, SKIPZ, float><<<grid, block, smem, st>>>(a, tb);
+      return;
+    }
+  } else {
+    if (a.tin == DT_F64) {
+      k_cols<W, SKIPZ, double><<<grid, block, smem, st>>>(a, tb);
+      return;
+    }
+  }
+  k_cols<W, SKIPZ, void><<<grid, block, smem, st>>>(a, tb);
+}
+
 // k_rows with typed loads for the input dtypes the fast kernels also take
 // (and float64 with double weights), runtime-typed loads for the rest
 template <class W, bool SKIPZ>
@@ -530,7 +548,6 @@ template <class W, bool SKIPZ>
 int launch_t(GArgs a, const TapBlock<W>& tb, bool direct, cudaStream_t st) {
   static std::once_flag once;
   std::call_once(once, [] {
-    allow_big_smem(k_cols<W, SKIPZ>);
     if constexpr (std::is_same<W, float>::value) allow_big_smem(k_cols_pairs<SKIPZ>);
   });
   const long long total = a.outer * a.L * a.inner;
@@ -561,7 +578,7 @@ int launch_t(GArgs a, const TapBlock<W>& tb, bool direct, cudaStream_t st) {
     a.tiles_a = (a.inner + kColTI - 1) / kColTI;
     a.tiles_b = (a.L + kColTL - 1) / kColTL;
     const long long blocks = a.tiles_a * a.tiles_b * a.outer;
-    k_cols<W, SKIPZ><<<(unsigned)blocks, dim3(kColTI, kColTY), smem, st>>>(a, tb);
+    launch_cols<W, SKIPZ>(a, tb, dim3((unsigned)blocks), dim3(kColTI, kColTY), smem, st);
   }
   return cuda_fail(cudaGetLastError(), "generic pass launch");
 }

@@ -1,6 +1,7 @@
-"""Lone passes along the last axis: correlate1d / convolve1d /
+"""The generic row and column kernels and lone passes along the last axis
+(correlate1d / convolve1d /
 gaussian_filter1d / uniform_filter1d along axis -1, and filters whose only
-pass besides the last axis is a leading one. Over float32 data the slab
+pass besides the last axis is a leading one). Over float32 data the slab
 kernel takes such a pass behind an identity y pass; every other pair runs
 on the generic row kernel (typed or runtime-typed loads, outputs stored
 straight or through the row buffer by their width). Either way the result
@@ -130,3 +131,22 @@ def test_last_axis_large_rows(ndi):
     xd = dev(x)
     got = host(ndi.gaussian_filter1d(xd, 2.0, axis=-1, output=np.float32))
     _same_bits(got, R.gaussian_filter1d(x, 2.0, axis=-1, output=np.float32))
+
+
+@pytest.mark.parametrize("tin,tout", [(np.float64, np.float64), (np.float32, np.float32),
+                                      (np.int16, np.float32), (np.int32, np.int32),
+                                      (np.uint16, np.uint16), (np.float64, np.float32)])
+@pytest.mark.parametrize("mode", MODES)
+def test_strided_axes_generic(ndi, tin, tout, mode):
+    """The generic strided-axis kernel: lines long enough for tiles inside
+    the line (walked, typed loads for float32 / float64) and tiles past
+    either end (the row table), every mode, through pass_by_pass so that no
+    fused kernel takes the fast pairs."""
+    x = _input((3, 300, 40), tin, 7)
+    xd = dev(x)
+    for axis, sigma in ((0, 1.0), (1, 1.5), (1, 6.0)):
+        exp = R.gaussian_filter1d(x, sigma, axis=axis, mode=mode, cval=2.5, output=tout)
+        with ndi.pass_by_pass():
+            got = host(ndi.gaussian_filter1d(xd, sigma, axis=axis, mode=mode, cval=2.5,
+                                              output=tout))
+        _same_bits(got, exp)
