@@ -516,11 +516,15 @@ __global__ void __launch_bounds__(Geom<T, KB>::NT, Geom<T, KB>::MINB) k_slab(con
   const int cr = clampi(a.X - xst, cl, G::RX);
   const int rl = clampi(-ys, 0, G::RY);
   const int rr = clampi(a.Y - ys, rl, G::RY);
-  // other inputs with a raw buffer of their own: a tile whose staged region
-  // lies inside the array skips the conversion to s_in, the y pass reads
-  // element pairs of the raw tile (the same for every thread of the CTA)
-  const bool direct = !G::F32 && G::SEP && TMA && rl == 0 && rr == G::RY && cl == 0 &&
-                      cr == G::RX;
+  // other inputs with a raw buffer of their own: the y pass reads element
+  // pairs of the raw tile and the conversion to s_in is skipped, for every
+  // tile whose staged elements outside the array can be patched in place
+  // with elements of the array: all of them but those with rows outside
+  // under a constant y mode (whose fill value need not fit in T); x-constant
+  // columns are replaced after the y pass (the same for every thread of the
+  // CTA)
+  const bool direct = !G::F32 && G::SEP && TMA &&
+                      ((rl == 0 && rr == G::RY) || my != CIMX_MODE_CONSTANT);
   // float input, or a direct tile: pairs are read from the TMA tile starting
   // at column off - sh (an even column)
   const int sh = ((TMA && G::F32) || direct) ? (off & 1) : 0;
@@ -561,12 +565,12 @@ __global__ void __launch_bounds__(Geom<T, KB>::NT, Geom<T, KB>::MINB) k_slab(con
     }
     if (!__syncthreads_and(ok)) return;
   }
-  if (G::F32 && TMA) {
-    // the tile is already float: rewrite only the staged elements that lie
-    // outside the array with their boundary-mode values
+  if ((G::F32 && TMA) || direct) {
+    // the y pass reads the raw tile: rewrite only the staged elements that
+    // lie outside the array with their boundary-mode values, as elements of T
     // (the same test for every thread of the CTA, so the barrier inside holds)
     if (!(rl == 0 && rr == G::RY && cl == 0 && cr == G::RX)) {
-      float* rawf = reinterpret_cast<float*>(raw);
+      T* rawf = raw;
       // Only the staged elements outside the array are visited, spread over
       // every thread of the CTA.
       // 1. rows inside the array: a column outside takes the value of the
@@ -578,15 +582,15 @@ __global__ void __launch_bounds__(Geom<T, KB>::NT, Geom<T, KB>::MINB) k_slab(con
       for (int t = threadIdx.x; t < n1; t += G::NT) {
         const int r = rl + t / nout, j = t % nout;
         const int c = j < nleft ? j : cr + (j - nleft);
-        float* row = rawf + r * G::BX + off;
+        T* row = rawf + r * G::BX + off;
         const long long xm = map_coord_near(xst + c, a.X, mx);
-        float v = 0.f;
+        T v = T(0);
         if (xm >= 0) {
           const long long sc = xm - xst;
           if (sc >= cl && sc < cr) {
             v = row[sc];
           } else {
-            v = static_cast<float>(in[(ys + r) * a.X + xm]);
+            v = in[(ys + r) * a.X + xm];
           }
         }
         row[c] = v;
@@ -599,21 +603,24 @@ __global__ void __launch_bounds__(Geom<T, KB>::NT, Geom<T, KB>::MINB) k_slab(con
       for (int t = threadIdx.x; t < n2; t += G::NT) {
         const int q = t / G::RX, c = t % G::RX;
         const int r = q < rl ? q : rr + (q - rl);
-        float* row = rawf + r * G::BX + off;
+        T* row = rawf + r * G::BX + off;
         const long long ym = map_coord_near(ys + r, a.Y, my);
         const long long sr = ym - ys;
-        float v;
+        T v;
         if (ym < 0) {
-          v = cy;
+          // float input only: a direct tile has no y-constant rows outside
+          if constexpr (G::F32) v = cy;
+          else v = T(0);
         } else if (sr >= rl && sr < rr) {
           v = rawf[sr * G::BX + off + c];
         } else {
-          v = staged_value<T>(in, ys + r, xst + c, a, my, mx, cy);
+          // an element of the array (exact in float), or 0 in an x-constant column
+          v = static_cast<T>(staged_value<T>(in, ys + r, xst + c, a, my, mx, cy));
         }
         row[c] = v;
       }
     }
-  } else if (!direct) {
+  } else {
     // convert to float into the staging buffer at column c (pairs aligned)
     float* dst = G::F32 ? reinterpret_cast<float*>(raw) : s_in;
     const int stride = G::F32 ? G::BX : G::RXS;

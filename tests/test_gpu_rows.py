@@ -150,3 +150,25 @@ def test_strided_axes_generic(ndi, tin, tout, mode):
             got = host(ndi.gaussian_filter1d(xd, sigma, axis=axis, mode=mode, cval=2.5,
                                               output=tout))
         _same_bits(got, exp)
+
+
+@pytest.mark.parametrize("tin,tout", [(np.uint16, np.uint16), (np.uint16, np.float32),
+                                      (np.uint8, np.uint8), (np.uint8, np.float32),
+                                      (np.uint8, np.uint16)])
+@pytest.mark.parametrize("ymode,xmode", [("reflect", "constant"), ("constant", "mirror"),
+                                         ("constant", "constant"), ("wrap", "nearest"),
+                                         ("mirror", "reflect"), ("nearest", "wrap")])
+def test_integer_slab_modes(ndi, tin, tout, ymode, xmode):
+    """The (y, x) slab kernel on 8/16-bit input with TMA-eligible rows (a
+    multiple of 16 bytes): tiles inside the array and tiles past every edge,
+    one mode per axis, a fill value that does not fit the input dtype; the
+    y pass reads the raw tile directly except where rows outside take a
+    constant fill."""
+    x = _input((2, 70, 272), tin, 8)
+    xd = dev(x)
+    for sigma in ((0, 0.7, 1.2), (0, 2.0, 4.0), (0, 5.0, 1.0)):
+        kw = dict(mode=("reflect", ymode, xmode), cval=3.5, output=tout)
+        got = host(ndi.gaussian_filter(xd, sigma, **kw))
+        _same_bits(got, R.gaussian_filter(x, sigma, **kw))
+        with ndi.pass_by_pass():
+            _same_bits(got, host(ndi.gaussian_filter(xd, sigma, **kw)))
