@@ -216,9 +216,10 @@ __global__ void __launch_bounds__(256, sizeof(W) == 4 ? 6 : 4) k_rows(GArgs a, T
 
 // Filter along a strided axis (inner > 1). Block = (32 inner columns, 8);
 // each thread produces P consecutive outputs of one column. With typed loads
-// (TI: float32 input with float weights, float64 with double weights; void:
-// runtime-typed) a tile inside the line walks its rows directly; otherwise
-// each staged row's mapped offset comes from a table built once per CTA.
+// (TI: float32 / uint16 / uint8 input with float weights, float64 with
+// double weights; void: runtime-typed) a tile inside the line walks its rows
+// directly; otherwise each staged row's mapped offset comes from a table
+// built once per CTA.
 template <class W, bool SKIPZ, class TI>
 __global__ void __launch_bounds__(256, sizeof(W) == 4 ? 6 : 4) k_cols(GArgs a, TapBlock<W> tb) {
   extern __shared__ __align__(16) unsigned char sm_raw[];
@@ -241,10 +242,10 @@ __global__ void __launch_bounds__(256, sizeof(W) == 4 ? 6 : 4) k_cols(GArgs a, T
   const W cv = fill_value<W>(a.cval, a.cval_as_input, a.tin);
   const long long obase = o * a.L;
   const bool interior = l0 - a.anchor >= 0 && l0 - a.anchor + span <= a.L;
-  // typed loads (float32 input with float weights, float64 with double):
-  // an interior tile walks its rows, eight loads in flight; the other
-  // dtypes take one runtime-typed load per row (measured: eight-wide
-  // staging of those made them 5-8 % slower, float64 1.6x faster)
+  // typed loads: an interior tile walks its rows, eight loads in flight;
+  // the other dtypes take one runtime-typed load per row (measured at six
+  // CTAs per SM: typed staging 1.6x faster for float64, 4-5 % for uint16 /
+  // uint8; eight-wide runtime-typed staging 5-8 % slower)
   constexpr bool kTyped = !std::is_void<TI>::value;
   const bool walk = interior && kTyped;
   if (!walk) {  // the same for every thread of the CTA
@@ -488,19 +489,32 @@ void allow_big_smem(Kern k) {
   cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem);
 }
 
-// k_cols with typed loads for float32 (float weights) and float64 input
+// k_cols with typed loads for float32 / uint16 / uint8 (float weights) and
+// float64 input
 template <class W, bool SKIPZ>
 void launch_cols(const GArgs& a, const TapBlock<W>& tb, dim3 grid, dim3 block, size_t smem,
                  cudaStream_t st) {
   static std::once_flag once;
   std::call_once(once, [] {
     allow_big_smem(k_cols<W, SKIPZ, void>);
-    if constexpr (std::is_same<W, float>::value) allow_big_smem(k_cols<W, SKIPZ, float>);
+    if constexpr (std::is_same<W, float>::value) {
+      allow_big_smem(k_cols<W, SKIPZ, float>);
+      allow_big_smem(k_cols<W, SKIPZ, uint16_t>);
+      allow_big_smem(k_cols<W, SKIPZ, uint8_t>);
+    }
     else allow_big_smem(k_cols<W, SKIPZ, double>);
   });
   if constexpr (std::is_same<W, float>::value) {
     if (a.tin == DT_F32) {
       k_cols<W, SKIPZ, float><<<grid, block, smem, st>>>(a, tb);
+      return;
+    }
+    if (a.tin == DT_U16) {
+      k_cols<W, SKIPZ, uint16_t><<<grid, block, smem, st>>>(a, tb);
+      return;
+    }
+    if (a.tin == DT_U8) {
+      k_cols<W, SKIPZ, uint8_t><<<grid, block, smem, st>>>(a, tb);
       return;
     }
   } else {

@@ -135,11 +135,13 @@ def test_last_axis_large_rows(ndi):
 
 @pytest.mark.parametrize("tin,tout", [(np.float64, np.float64), (np.float32, np.float32),
                                       (np.int16, np.float32), (np.int32, np.int32),
-                                      (np.uint16, np.uint16), (np.float64, np.float32)])
+                                      (np.uint16, np.uint16), (np.float64, np.float32),
+                                      (np.uint8, np.uint8), (np.uint8, np.float32),
+                                      (np.uint16, np.float32)])
 @pytest.mark.parametrize("mode", MODES)
 def test_strided_axes_generic(ndi, tin, tout, mode):
     """The generic strided-axis kernel: lines long enough for tiles inside
-    the line (walked, typed loads for float32 / float64) and tiles past
+    the line (walked, typed loads for float32 / uint16 / uint8 / float64) and tiles past
     either end (the row table), every mode, through pass_by_pass so that no
     fused kernel takes the fast pairs."""
     x = _input((3, 300, 40), tin, 7)
