@@ -284,7 +284,9 @@ int launch_stream_td(const PassDesc& d, const float* w, int K, int anchor, bool 
     case 5: return launch_stream_k<T, D, 5>(d, w, anchor, interior_zero, in, out, st);
     case 7: return launch_stream_k<T, D, 7>(d, w, anchor, interior_zero, in, out, st);
     case 9: return launch_stream_k<T, D, 9>(d, w, anchor, interior_zero, in, out, st);
+    case 11: return launch_stream_k<T, D, 11>(d, w, anchor, interior_zero, in, out, st);
     case 13: return launch_stream_k<T, D, 13>(d, w, anchor, interior_zero, in, out, st);
+    case 15: return launch_stream_k<T, D, 15>(d, w, anchor, interior_zero, in, out, st);
     case 17: return launch_stream_k<T, D, 17>(d, w, anchor, interior_zero, in, out, st);
     default: return CIMX_FUSED_DECLINED;
   }

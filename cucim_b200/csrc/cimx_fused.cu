@@ -27,8 +27,11 @@ bool fast_pair(int t, int d) {
   }
 }
 
+// tap counts of the stream kernel's instantiations: the gaussians of
+// sigma 0.5 / 0.75 / 1 / 1.25 / 1.5 / 1.75 / 2 (truncate 4) and the short
+// box and derivative filters
 bool stream_supports(int K) {
-  return K == 3 || K == 5 || K == 7 || K == 9 || K == 13 || K == 17;
+  return K == 3 || K == 5 || K == 7 || K == 9 || K == 11 || K == 13 || K == 15 || K == 17;
 }
 
 struct Trimmed {
