@@ -54,7 +54,7 @@ int try_fused(const CimxArray* in, const CimxArray* out, PassDesc* ds, int npass
 int launch_copy_cast(const void* in, int tin, void* out, int tout, int64_t n,
                      cudaStream_t stream);
 
-// stream pass along a strided axis, by input dtype; K in {3,5,7,9,11,13,15,17}
+// stream pass along a strided axis, by input dtype; K in {3,5,...,17} (odd)
 int launch_stream_f32(const PassDesc& d, const float* w, int K, int anchor, bool interior_zero,
                       const void* in, int tout, void* out, cudaStream_t st);
 int launch_stream_u16(const PassDesc& d, const float* w, int K, int anchor, bool interior_zero,

@@ -269,13 +269,13 @@ def test_passes_out_of_axis_order(ndi, axes, tin, tout):
         np.testing.assert_array_equal(again, exp)
 
 
-@pytest.mark.parametrize("taps", [3, 5, 7, 9, 11, 13, 15, 17, 19])
+@pytest.mark.parametrize("taps", [3, 5, 7, 9, 11, 13, 15, 17, 19, 21, 23, 25])
 @pytest.mark.parametrize("tin,tout", [(np.uint16, np.float32), (np.uint16, np.uint16),
                                       (np.float32, np.float32), (np.uint8, np.uint8)])
 @pytest.mark.parametrize("mode", MODES)
 def test_stream_tap_counts(ndi, taps, tin, tout, mode):
     """A pass along a leading axis at every tap count the stream kernel is
-    instantiated for (19: one it is not, on the generic kernel), uneven
+    instantiated for (19 and above: the generic kernel), uneven
     taps with an origin, against the oracle and the generic schedule."""
     x = _ints((23, 6, 40), tin, 30 + taps, hi=250)
     w = np.linspace(-0.4, 0.9, taps)
