@@ -354,7 +354,7 @@ __device__ __forceinline__ void tap_loop_pairs(u64 (&acc)[P], const u64* taps, i
   }
 }
 
-// k_cols for float32 input and float32 taps: block = (16 column pairs, 16);
+// k_cols for float32 taps over float32 / uint16 / uint8 input: block = (16 column pairs, 16);
 // each thread produces P consecutive outputs of two adjacent columns with
 // one f32x2 FMA per tap and output pair, and a tile is 32 columns x 128
 // outputs (half the halo share of k_cols' 64-output tiles). Four CTAs per
@@ -363,7 +363,9 @@ __device__ __forceinline__ void tap_loop_pairs(u64 (&acc)[P], const u64* taps, i
 // table of row offsets in shared memory) rather than per element, which
 // took a fifth of the time off every pass. 256^3 float32, axis 0: 70, 95
 // and 152 us at 23, 57 and 143 taps, against 89, 129 and 242 us for k_cols.
-template <bool SKIPZ>
+// TI: the input element type (float32, or uint16 / uint8 widened exactly
+// to float32 as they are staged).
+template <bool SKIPZ, class TI>
 __global__ void __launch_bounds__(256, 4) k_cols_pairs(GArgs a, TapBlock<float> tb) {
   extern __shared__ __align__(16) unsigned char sm_raw[];
   u64* taps = reinterpret_cast<u64*>(sm_raw);
@@ -401,7 +403,7 @@ __global__ void __launch_bounds__(256, 4) k_cols_pairs(GArgs a, TapBlock<float> 
     // loads in flight before the stores
     const int c = tid & 31, r = tid >> 5;
     const long long ic = it * 32 + c;
-    const float* col = static_cast<const float*>(a.in) + obase * a.inner + ic;
+    const TI* col = static_cast<const TI*>(a.in) + obase * a.inner + ic;
     const bool cin = ic < a.inner;
     for (int jb = r; jb < span; jb += 64) {
       float v[8];
@@ -411,7 +413,7 @@ __global__ void __launch_bounds__(256, 4) k_cols_pairs(GArgs a, TapBlock<float> 
         v[q] = 0.f;
         if (j < span && cin) {
           const long long off = rowoff[j];
-          v[q] = off < 0 ? cv : __ldg(col + off);
+          v[q] = off < 0 ? cv : static_cast<float>(__ldg(col + off));
         }
       }
 #pragma unroll
@@ -562,7 +564,11 @@ template <class W, bool SKIPZ>
 int launch_t(GArgs a, const TapBlock<W>& tb, bool direct, cudaStream_t st) {
   static std::once_flag once;
   std::call_once(once, [] {
-    if constexpr (std::is_same<W, float>::value) allow_big_smem(k_cols_pairs<SKIPZ>);
+    if constexpr (std::is_same<W, float>::value) {
+      allow_big_smem(k_cols_pairs<SKIPZ, float>);
+      allow_big_smem(k_cols_pairs<SKIPZ, uint16_t>);
+      allow_big_smem(k_cols_pairs<SKIPZ, uint8_t>);
+    }
   });
   const long long total = a.outer * a.L * a.inner;
   if (total == 0) return CIMX_OK;
@@ -576,14 +582,19 @@ int launch_t(GArgs a, const TapBlock<W>& tb, bool direct, cudaStream_t st) {
     launch_rows<W, SKIPZ>(a, tb, dim3((unsigned)blocks), dim3(g.seg_threads, g.ry), g.smem, st);
   } else {
     if constexpr (std::is_same<W, float>::value) {
-      // float32 input along lines longer than one k_cols tile: column pairs
+      // float32 / uint16 / uint8 input (float32 taps) along lines longer than one
+      // k_cols tile: column pairs
       const size_t span2 = (size_t)(kCol2TL + a.K8 + P);
       const size_t smem2 = 8 * (size_t)a.K8 + sizeof(float) * span2 * 32 + 8 * span2;
-      if (a.tin == DT_F32 && a.inner >= 2 && a.L > kColTL && smem2 <= (size_t)kMaxSmem) {
+      const bool pair_in = a.tin == DT_F32 || a.tin == DT_U16 || a.tin == DT_U8;
+      if (pair_in && a.inner >= 2 && a.L > kColTL && smem2 <= (size_t)kMaxSmem) {
         a.tiles_a = (a.inner + 31) / 32;
         a.tiles_b = (a.L + kCol2TL - 1) / kCol2TL;
         const long long blocks = a.tiles_a * a.tiles_b * a.outer;
-        k_cols_pairs<SKIPZ><<<(unsigned)blocks, dim3(16, kCol2TY), smem2, st>>>(a, tb);
+        const dim3 grid((unsigned)blocks), block(16, kCol2TY);
+        if (a.tin == DT_F32) k_cols_pairs<SKIPZ, float><<<grid, block, smem2, st>>>(a, tb);
+        else if (a.tin == DT_U16) k_cols_pairs<SKIPZ, uint16_t><<<grid, block, smem2, st>>>(a, tb);
+        else k_cols_pairs<SKIPZ, uint8_t><<<grid, block, smem2, st>>>(a, tb);
         return cuda_fail(cudaGetLastError(), "generic pass launch");
       }
     }

@@ -1,4 +1,4 @@
-"""GPU parity of the column-pair pass (float32 input along a strided axis of
+"""GPU parity of the column-pair pass (float32, uint16 or uint8 input along a strided axis of
 lines longer than 64 samples): bit for bit against the oracle at the tile
 edges (lines of 65, 128, 129 and 257 samples), with an odd number of
 columns (the last pair has one column), two columns, several outer slabs,
@@ -70,3 +70,21 @@ def test_cols_pairs_matches_single_columns(ndi):
     a = ndi.correlate1d(xd, w, 0, mode="nearest").cpu().numpy()
     b = ndi.correlate1d(xd.T.contiguous(), w, 1, mode="nearest").cpu().numpy().T
     np.testing.assert_array_equal(a, b)
+
+
+@pytest.mark.parametrize("dtype", [np.uint16, np.uint8])
+@pytest.mark.parametrize("shape", [(65, 33), (129, 35), (3, 200, 9)])
+@pytest.mark.parametrize("mode", MODES)
+@pytest.mark.parametrize("K", [23, 57])
+def test_cols_pairs_integer_input(ndi, dtype, shape, mode, K):
+    """uint16 / uint8 input, widened exactly to float32 as it is staged,
+    with the input dtype and float32 as outputs and a fill value that does
+    not fit the input dtype."""
+    rng = np.random.default_rng(K + len(shape) + 7)
+    hi = np.iinfo(dtype).max
+    x = rng.integers(0, hi + 1, shape).astype(dtype)
+    w = rng.standard_normal(K).astype(np.float32) / 8
+    axis = len(shape) - 2
+    for output in (dtype, np.float32):
+        for origin in (0, K // 2):
+            _run(ndi, x, w, axis, mode=mode, cval=-3.25, origin=origin, output=output)
