@@ -354,7 +354,7 @@ __device__ __forceinline__ void tap_loop_pairs(u64 (&acc)[P], const u64* taps, i
   }
 }
 
-// k_cols for float32 taps over float32 / uint16 / uint8 input: block = (16 column pairs, 16);
+// k_cols for float32 input and float32 taps: block = (16 column pairs, 16);
 // each thread produces P consecutive outputs of two adjacent columns with
 // one f32x2 FMA per tap and output pair, and a tile is 32 columns x 128
 // outputs (half the halo share of k_cols' 64-output tiles). Four CTAs per
@@ -582,11 +582,14 @@ int launch_t(GArgs a, const TapBlock<W>& tb, bool direct, cudaStream_t st) {
     launch_rows<W, SKIPZ>(a, tb, dim3((unsigned)blocks), dim3(g.seg_threads, g.ry), g.smem, st);
   } else {
     if constexpr (std::is_same<W, float>::value) {
-      // float32 / uint16 / uint8 input (float32 taps) along lines longer than one
-      // k_cols tile: column pairs
+      // float32 input (float32 taps) along lines longer than one k_cols tile:
+      // column pairs
       const size_t span2 = (size_t)(kCol2TL + a.K8 + P);
       const size_t smem2 = 8 * (size_t)a.K8 + sizeof(float) * span2 * 32 + 8 * span2;
-      const bool pair_in = a.tin == DT_F32 || a.tin == DT_U16 || a.tin == DT_U8;
+      // float32 input only: uint16 / uint8 input measured slower here than on
+      // the typed k_cols for short taps (9 taps, 256 x 512^2 along axis 0:
+      // 374 / 353 us against 350 / 338 us) and within 0-4 % for 21-33 taps
+      const bool pair_in = a.tin == DT_F32;
       if (pair_in && a.inner >= 2 && a.L > kColTL && smem2 <= (size_t)kMaxSmem) {
         a.tiles_a = (a.inner + 31) / 32;
         a.tiles_b = (a.L + kCol2TL - 1) / kCol2TL;

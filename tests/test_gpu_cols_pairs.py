@@ -1,4 +1,4 @@
-"""GPU parity of the column-pair pass (float32, uint16 or uint8 input along a strided axis of
+"""GPU parity of the column-pair pass (float32 input along a strided axis of
 lines longer than 64 samples): bit for bit against the oracle at the tile
 edges (lines of 65, 128, 129 and 257 samples), with an odd number of
 columns (the last pair has one column), two columns, several outer slabs,
@@ -77,7 +77,7 @@ def test_cols_pairs_matches_single_columns(ndi):
 @pytest.mark.parametrize("mode", MODES)
 @pytest.mark.parametrize("K", [23, 57])
 def test_cols_pairs_integer_input(ndi, dtype, shape, mode, K):
-    """uint16 / uint8 input, widened exactly to float32 as it is staged,
+    """uint16 / uint8 input on the same lines (the typed column kernel),
     with the input dtype and float32 as outputs and a fill value that does
     not fit the input dtype."""
     rng = np.random.default_rng(K + len(shape) + 7)
