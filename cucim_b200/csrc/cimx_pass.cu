@@ -216,10 +216,9 @@ __global__ void __launch_bounds__(256, sizeof(W) == 4 ? 6 : 4) k_rows(GArgs a, T
 
 // Filter along a strided axis (inner > 1). Block = (32 inner columns, 8);
 // each thread produces P consecutive outputs of one column. With typed loads
-// (TI: float32 / uint16 / uint8 input with float weights, float64 with
-// double weights; void: runtime-typed) a tile inside the line walks its rows
-// directly; otherwise each staged row's mapped offset comes from a table
-// built once per CTA.
+// (TI: see with_input_type; void: runtime-typed) a tile inside the line
+// walks its rows directly; otherwise each staged row's mapped offset comes
+// from a table built once per CTA.
 template <class W, bool SKIPZ, class TI>
 __global__ void __launch_bounds__(256, sizeof(W) == 4 ? 6 : 4) k_cols(GArgs a, TapBlock<W> tb) {
   extern __shared__ __align__(16) unsigned char sm_raw[];
@@ -491,73 +490,49 @@ void allow_big_smem(Kern k) {
   cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem);
 }
 
-// k_cols with typed loads for float32 / uint16 / uint8 (float weights) and
-// float64 input
-template <class W, bool SKIPZ>
-void launch_cols(const GArgs& a, const TapBlock<W>& tb, dim3 grid, dim3 block, size_t smem,
-                 cudaStream_t st) {
-  static std::once_flag once;
-  std::call_once(once, [] {
-    allow_big_smem(k_cols<W, SKIPZ, void>);
-    if constexpr (std::is_same<W, float>::value) {
-      allow_big_smem(k_cols<W, SKIPZ, float>);
-      allow_big_smem(k_cols<W, SKIPZ, uint16_t>);
-      allow_big_smem(k_cols<W, SKIPZ, uint8_t>);
-    }
-    else allow_big_smem(k_cols<W, SKIPZ, double>);
-  });
+// The input dtypes with typed loads in k_cols / k_rows: float32, uint16,
+// uint8 and int16 with float weights, float64 and int32 with double weights;
+// the others are loaded by their runtime dtype code (TI = void).
+template <class W, class F>
+void with_input_type(int dt, F&& f) {
   if constexpr (std::is_same<W, float>::value) {
-    if (a.tin == DT_F32) {
-      k_cols<W, SKIPZ, float><<<grid, block, smem, st>>>(a, tb);
-      return;
-    }
-    if (a.tin == DT_U16) {
-      k_cols<W, SKIPZ, uint16_t><<<grid, block, smem, st>>>(a, tb);
-      return;
-    }
-    if (a.tin == DT_U8) {
-      k_cols<W, SKIPZ, uint8_t><<<grid, block, smem, st>>>(a, tb);
-      return;
-    }
-  } else {
-    if (a.tin == DT_F64) {
-      k_cols<W, SKIPZ, double><<<grid, block, smem, st>>>(a, tb);
-      return;
-    }
-  }
-  k_cols<W, SKIPZ, void><<<grid, block, smem, st>>>(a, tb);
-}
-
-// k_rows with typed loads for the input dtypes the fast kernels also take
-// (and float64 with double weights), runtime-typed loads for the rest
-template <class W, bool SKIPZ>
-void launch_rows(const GArgs& a, const TapBlock<W>& tb, dim3 grid, dim3 block, size_t smem,
-                 cudaStream_t st) {
-  static std::once_flag once;
-  std::call_once(once, [] {
-    allow_big_smem(k_rows<W, SKIPZ, void>);
-    if constexpr (std::is_same<W, float>::value) {
-      allow_big_smem(k_rows<W, SKIPZ, float>);
-      allow_big_smem(k_rows<W, SKIPZ, uint16_t>);
-      allow_big_smem(k_rows<W, SKIPZ, uint8_t>);
-    } else {
-      allow_big_smem(k_rows<W, SKIPZ, double>);
-    }
-  });
-  if constexpr (std::is_same<W, float>::value) {
-    switch (a.tin) {
-      case DT_F32: k_rows<W, SKIPZ, float><<<grid, block, smem, st>>>(a, tb); return;
-      case DT_U16: k_rows<W, SKIPZ, uint16_t><<<grid, block, smem, st>>>(a, tb); return;
-      case DT_U8: k_rows<W, SKIPZ, uint8_t><<<grid, block, smem, st>>>(a, tb); return;
+    switch (dt) {
+      case DT_F32: f(static_cast<float*>(nullptr)); return;
+      case DT_U16: f(static_cast<uint16_t*>(nullptr)); return;
+      case DT_U8: f(static_cast<uint8_t*>(nullptr)); return;
+      case DT_I16: f(static_cast<int16_t*>(nullptr)); return;
       default: break;
     }
   } else {
-    if (a.tin == DT_F64) {
-      k_rows<W, SKIPZ, double><<<grid, block, smem, st>>>(a, tb);
-      return;
+    switch (dt) {
+      case DT_F64: f(static_cast<double*>(nullptr)); return;
+      case DT_I32: f(static_cast<int32_t*>(nullptr)); return;
+      default: break;
     }
   }
-  k_rows<W, SKIPZ, void><<<grid, block, smem, st>>>(a, tb);
+  f(static_cast<void*>(nullptr));
+}
+
+template <class W, bool SKIPZ>
+void launch_cols(const GArgs& a, const TapBlock<W>& tb, dim3 grid, dim3 block, size_t smem,
+                 cudaStream_t st) {
+  with_input_type<W>(a.tin, [&](auto* tag) {
+    using TI = std::remove_pointer_t<decltype(tag)>;
+    static std::once_flag once;
+    std::call_once(once, [] { allow_big_smem(k_cols<W, SKIPZ, TI>); });
+    k_cols<W, SKIPZ, TI><<<grid, block, smem, st>>>(a, tb);
+  });
+}
+
+template <class W, bool SKIPZ>
+void launch_rows(const GArgs& a, const TapBlock<W>& tb, dim3 grid, dim3 block, size_t smem,
+                 cudaStream_t st) {
+  with_input_type<W>(a.tin, [&](auto* tag) {
+    using TI = std::remove_pointer_t<decltype(tag)>;
+    static std::once_flag once;
+    std::call_once(once, [] { allow_big_smem(k_rows<W, SKIPZ, TI>); });
+    k_rows<W, SKIPZ, TI><<<grid, block, smem, st>>>(a, tb);
+  });
 }
 
 template <class W, bool SKIPZ>
