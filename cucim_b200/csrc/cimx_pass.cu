@@ -490,23 +490,27 @@ void allow_big_smem(Kern k) {
   cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem);
 }
 
-// The input dtypes with typed loads in k_cols / k_rows: float32, uint16,
-// uint8 and int16 with float weights, float64 and int32 with double weights;
-// the others are loaded by their runtime dtype code (TI = void).
+// The input dtypes with typed loads in k_cols / k_rows: float32, float16,
+// uint16, int16, uint8 and int8 with float weights, float64, int32 and
+// uint32 with double weights; the 64-bit integers are loaded by their
+// runtime dtype code (TI = void).
 template <class W, class F>
 void with_input_type(int dt, F&& f) {
   if constexpr (std::is_same<W, float>::value) {
     switch (dt) {
       case DT_F32: f(static_cast<float*>(nullptr)); return;
+      case DT_F16: f(static_cast<__half*>(nullptr)); return;
       case DT_U16: f(static_cast<uint16_t*>(nullptr)); return;
-      case DT_U8: f(static_cast<uint8_t*>(nullptr)); return;
       case DT_I16: f(static_cast<int16_t*>(nullptr)); return;
+      case DT_U8: f(static_cast<uint8_t*>(nullptr)); return;
+      case DT_I8: f(static_cast<int8_t*>(nullptr)); return;
       default: break;
     }
   } else {
     switch (dt) {
       case DT_F64: f(static_cast<double*>(nullptr)); return;
       case DT_I32: f(static_cast<int32_t*>(nullptr)); return;
+      case DT_U32: f(static_cast<uint32_t*>(nullptr)); return;
       default: break;
     }
   }

@@ -21,7 +21,8 @@ MODES = ["reflect", "mirror", "nearest", "wrap", "constant"]
 SHAPES = [(33, 128), (7, 9, 244), (5, 70), (3, 4, 37), (17, 8), (2, 1, 100), (1, 3)]
 PAIRS = [(np.float32, np.float32), (np.uint16, np.float32), (np.uint16, np.uint16),
          (np.uint8, np.uint8), (np.uint8, np.float32), (np.uint8, np.uint16),
-         (np.float64, np.float64), (np.int16, np.float32)]
+         (np.float64, np.float64), (np.int16, np.float32), (np.float16, np.float32),
+         (np.int32, np.float64)]
 
 
 def dev(a):
@@ -53,7 +54,7 @@ def _same_bits(got, exp):
     if got.dtype.kind == "f":
         nan = np.isnan(exp)
         assert np.array_equal(np.isnan(got), nan)
-        u = np.uint32 if got.dtype.itemsize == 4 else np.uint64
+        u = {2: np.uint16, 4: np.uint32, 8: np.uint64}[got.dtype.itemsize]
         np.testing.assert_array_equal(got.view(u)[~nan], exp.view(u)[~nan])
     else:
         np.testing.assert_array_equal(got, exp)
@@ -137,7 +138,9 @@ def test_last_axis_large_rows(ndi):
                                       (np.int16, np.float32), (np.int32, np.int32),
                                       (np.uint16, np.uint16), (np.float64, np.float32),
                                       (np.uint8, np.uint8), (np.uint8, np.float32),
-                                      (np.uint16, np.float32)])
+                                      (np.uint16, np.float32), (np.float16, np.float16),
+                                      (np.float16, np.float32), (np.int8, np.int8),
+                                      (np.uint32, np.uint32), (np.int16, np.int16)])
 @pytest.mark.parametrize("mode", MODES)
 def test_strided_axes_generic(ndi, tin, tout, mode):
     """The generic strided-axis kernel: lines long enough for tiles inside
