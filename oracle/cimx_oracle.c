@@ -424,6 +424,28 @@ void oracle_cast(const void* in, int w64, void* out, int tout, int64_t n) {
   }
 }
 
+/* The fold of cuCIM's min / max kernels: CUDA's fmin / fmax on the GPU,
+ * which behave as IEEE 754-2019 minimumNumber / maximumNumber: a nan
+ * operand is ignored (nan only if both are), and -0 orders below +0 whatever
+ * the operand order. (The C library's fmin / fmax may return either zero
+ * for a pair of opposite-signed zeros; glibc returns the second operand.)
+ * Checked against the GPU output on windows that mix -0 and +0. */
+static double min_number(double a, double b) {
+  if (isnan(a)) return b;
+  if (isnan(b)) return a;
+  if (a < b) return a;
+  if (b < a) return b;
+  return signbit(a) ? a : b;
+}
+
+static double max_number(double a, double b) {
+  if (isnan(a)) return b;
+  if (isnan(b)) return a;
+  if (a > b) return a;
+  if (b > a) return b;
+  return signbit(a) ? b : a;
+}
+
 /* minimum_filter1d / maximum_filter1d (_vendored/_ndimage_filters.py:1362-1497,
  * _get_min_or_max_kernel without weights): value = x[l] as a double, then
  * every window element in order folded with fmin / fmax (cval outside the
@@ -438,7 +460,7 @@ void oracle_min_max1d(const void* in, int tin, void* out, int tout, int64_t oute
         for (int k = 0; k < size; ++k) {
           const int64_t m = map_index(l - anchor + k, L, mode);
           const double v = m < 0 ? cval : load_d(in, tin, base + m * inner);
-          value = is_max ? fmax(v, value) : fmin(v, value);
+          value = is_max ? max_number(v, value) : min_number(v, value);
         }
         store_cast(out, tout, base + l * inner, value, 1);
       }

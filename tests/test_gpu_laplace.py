@@ -187,3 +187,33 @@ def test_generic_gradient_magnitude_user_callable(ndi, dtype):
     exp = R.generic_gradient_magnitude(x, R.prewitt, axes=(0, 2), mode=("mirror", "constant"),
                                        cval=2.0)
     np.testing.assert_array_equal(got, exp)
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64, np.uint16, np.int16])
+@pytest.mark.parametrize("mode", ["reflect", "constant", "wrap"])
+def test_min_max_filter1d_tiles(ndi, dtype, mode):
+    """The shared-memory tiles: rows longer than one 1024-output segment,
+    columns over several 32 x 64 tiles, windows from 2 to 80 elements;
+    signed zeros and nan runs in the float inputs (the fold keeps the
+    element-first, tap-ordered fmin / fmax of the reference kernel)."""
+    x = _data((2, 90, 1100), dtype)
+    if np.dtype(dtype).kind == "f":
+        x[0, 5, 100:140] = -0.0
+        x[0, 6, 100:140] = 0.0
+        x[1, 7, 1000:1010] = np.nan
+        x[1, 20:40, 33] = np.nan
+    xd = dev(x)
+    for axis in (2, 1, 0):
+        for size, origin in [(2, 0), (15, 3), (80, -30)]:
+            for name in ("minimum_filter1d", "maximum_filter1d"):
+                got = host(getattr(ndi, name)(xd, size, axis, mode=mode, cval=-1.5,
+                                              origin=origin))
+                exp = getattr(R, name)(x, size, axis, mode=mode, cval=-1.5, origin=origin)
+                assert got.dtype == exp.dtype
+                if got.dtype.kind == "f":
+                    u = np.uint32 if got.dtype.itemsize == 4 else np.uint64
+                    nan = np.isnan(exp)
+                    assert np.array_equal(np.isnan(got), nan)
+                    np.testing.assert_array_equal(got.view(u)[~nan], exp.view(u)[~nan])
+                else:
+                    np.testing.assert_array_equal(got, exp)
