@@ -35,21 +35,55 @@ constexpr int kRowT = 256, kRowP = 4, kRowSeg = kRowT * kRowP;  // 1024 outputs 
 constexpr int kColTI = 32, kColTY = 8, kColP = 8, kColTL = kColTY * kColP;  // 32 x 64 tile
 constexpr int kMaxSmem = 227 * 1024;
 
-__device__ __forceinline__ double fold(double v, double value, int is_max) {
+template <class F>
+__device__ __forceinline__ F fold(F v, F value, int is_max) {
   return is_max ? fmax(v, value) : fmin(v, value);
 }
 
-// Staged value of line coordinate c (boundary map outside [0, L)).
-__device__ __forceinline__ double staged(const MinMaxArgs& a, long long line0, long long c,
-                                         long long stride) {
+// Staged value of line coordinate c (boundary map outside [0, L)), as F.
+template <class F>
+__device__ __forceinline__ F staged(const MinMaxArgs& a, long long line0, long long c,
+                                    long long stride) {
   const long long m = (c >= 0 && c < a.L) ? c : map_coord_near(c, a.L, a.mode);
-  return m < 0 ? a.cval : load_as<double>(a.in, line0 + m * stride, a.tin);
+  return m < 0 ? static_cast<F>(a.cval) : load_as<F>(a.in, line0 + m * stride, a.tin);
+}
+
+// Folds P consecutive outputs: value[j] starts at window element j + anchor
+// (the output's own input element) and takes window elements j + k, k = 0 ..
+// size - 1, in order. `at(q)` returns window element q; the window slides in
+// registers, reloaded once per P taps.
+template <int P, class F, class At>
+__device__ __forceinline__ void fold_block(F (&value)[P], int size, int anchor, int is_max,
+                                           At at) {
+#pragma unroll
+  for (int j = 0; j < P; ++j) value[j] = at(j + anchor);
+  F win[2 * P];
+#pragma unroll
+  for (int j = 0; j < P; ++j) win[j] = at(j);
+  for (int k0 = 0; k0 < size; k0 += P) {
+#pragma unroll
+    for (int j = 0; j < P; ++j) win[P + j] = at(k0 + P + j);
+#pragma unroll
+    for (int kk = 0; kk < P; ++kk) {
+      if (k0 + kk < size) {
+#pragma unroll
+        for (int j = 0; j < P; ++j) value[j] = fold(win[j + kk], value[j], is_max);
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < P; ++j) win[j] = win[P + j];
+  }
 }
 
 // Last axis (inner == 1): one CTA per 1024 outputs of a row; thread t folds
-// outputs t, t + 256, t + 512, t + 768 of the segment (coalesced stores).
+// outputs 4t .. 4t + 3 of the segment. The staged stretch is padded by one
+// double every 4, so that lanes reading at a stride of 4 hit distinct banks.
+__device__ __forceinline__ int pad4(int j) { return j + (j >> 2); }
+
+template <class F>
 __global__ void __launch_bounds__(kRowT) k_minmax_rows(const MinMaxArgs a) {
-  extern __shared__ double s_line[];
+  extern __shared__ __align__(16) unsigned char s_raw_rows[];
+  F* s_line = reinterpret_cast<F*>(s_raw_rows);
   const long long row = blockIdx.x / a.tiles_b;
   const long long x0 = (blockIdx.x % a.tiles_b) * kRowSeg;
   const long long base = row * a.L;
@@ -57,23 +91,24 @@ __global__ void __launch_bounds__(kRowT) k_minmax_rows(const MinMaxArgs a) {
   const long long need = a.L - x0 + a.size - 1;
   const int n = need < kRowSeg + a.size - 1 ? static_cast<int>(need) : kRowSeg + a.size - 1;
   const long long c0 = x0 - a.anchor;
-  for (int j = threadIdx.x; j < n; j += kRowT) s_line[j] = staged(a, base, c0 + j, 1);
+  for (int j = threadIdx.x; j < n; j += kRowT) s_line[pad4(j)] = staged<F>(a, base, c0 + j, 1);
   __syncthreads();
+  const int lx = kRowP * threadIdx.x;
+  if (x0 + lx >= a.L) return;
+  F value[kRowP];
+  fold_block<kRowP>(value, a.size, a.anchor, a.is_max,
+                    [&](int q) { return s_line[pad4(lx + q)]; });
 #pragma unroll
-  for (int p = 0; p < kRowP; ++p) {
-    const int lx = threadIdx.x + p * kRowT;
-    if (x0 + lx >= a.L) break;
-    const double* w = s_line + lx;
-    double value = w[a.anchor];
-    for (int k = 0; k < a.size; ++k) value = fold(w[k], value, a.is_max);
-    store_cast<double>(a.out, base + x0 + lx, value, a.tout);
-  }
+  for (int j = 0; j < kRowP; ++j)
+    if (x0 + lx + j < a.L) store_cast<F>(a.out, base + x0 + lx + j, value[j], a.tout);
 }
 
 // Strided axis (inner > 1): a tile of 32 columns x 64 outputs; thread
-// (x, y) folds outputs y, y + 8, ..., y + 56 of column x.
+// (x, y) folds outputs 8y .. 8y + 7 of column x.
+template <class F>
 __global__ void __launch_bounds__(kColTI * kColTY) k_minmax_cols(const MinMaxArgs a) {
-  extern __shared__ double s_tile[];
+  extern __shared__ __align__(16) unsigned char s_raw_cols[];
+  F* s_tile = reinterpret_cast<F*>(s_raw_cols);
   long long bid = blockIdx.x;
   const long long it = bid % a.tiles_a;
   bid /= a.tiles_a;
@@ -85,18 +120,17 @@ __global__ void __launch_bounds__(kColTI * kColTY) k_minmax_cols(const MinMaxArg
   const int n = need < kColTL + a.size - 1 ? static_cast<int>(need) : kColTL + a.size - 1;
   const bool col_in = i < a.inner;
   for (int j = threadIdx.y; j < n; j += kColTY)
-    s_tile[j * kColTI + threadIdx.x] = col_in ? staged(a, line0, l0 - a.anchor + j, a.inner) : 0.0;
+    s_tile[j * kColTI + threadIdx.x] = col_in ? staged<F>(a, line0, l0 - a.anchor + j, a.inner) : F(0);
   __syncthreads();
-  if (!col_in) return;
+  const int ly = kColP * threadIdx.y;
+  if (!col_in || l0 + ly >= a.L) return;
+  F value[kColP];
+  fold_block<kColP>(value, a.size, a.anchor, a.is_max,
+                    [&](int q) { return s_tile[(ly + q) * kColTI + threadIdx.x]; });
 #pragma unroll
-  for (int p = 0; p < kColP; ++p) {
-    const int ly = threadIdx.y + p * kColTY;
-    if (l0 + ly >= a.L) break;
-    const double* w = s_tile + ly * kColTI + threadIdx.x;
-    double value = w[a.anchor * kColTI];
-    for (int k = 0; k < a.size; ++k) value = fold(w[k * kColTI], value, a.is_max);
-    store_cast<double>(a.out, line0 + (l0 + ly) * a.inner, value, a.tout);
-  }
+  for (int j = 0; j < kColP; ++j)
+    if (l0 + ly + j < a.L)
+      store_cast<F>(a.out, line0 + (l0 + ly + j) * a.inner, value[j], a.tout);
 }
 
 __global__ void __launch_bounds__(256) k_minmax1d(const MinMaxArgs a) {
@@ -156,17 +190,40 @@ extern "C" int cimx_min_max_1d(const CimxArray* in, const CimxArray* out, int si
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   static std::once_flag once;
   std::call_once(once, [] {
-    cudaFuncSetAttribute(k_minmax_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem);
-    cudaFuncSetAttribute(k_minmax_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxSmem);
+    cudaFuncSetAttribute(k_minmax_rows<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         kMaxSmem);
+    cudaFuncSetAttribute(k_minmax_cols<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         kMaxSmem);
+    cudaFuncSetAttribute(k_minmax_rows<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         kMaxSmem);
+    cudaFuncSetAttribute(k_minmax_cols<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         kMaxSmem);
   });
+  // The fold is exact in float32 when every value it sees is: inputs of at
+  // most float32 precision, and a fill value that float32 holds (or none).
+  // Rounding is monotonic, so the float32 min / max of the rounded values is
+  // the rounding of the float64 one, the same real number, stored with the
+  // same cast; nan and the zeros' signs behave alike in both precisions.
+  const int tin = in->dtype;
+  const bool f32_in = tin == DT_U8 || tin == DT_I8 || tin == DT_U16 || tin == DT_I16 ||
+                      tin == DT_F16 || tin == DT_F32;
+  const bool fill_exact = mode != CIMX_MODE_CONSTANT ||
+                          static_cast<double>(static_cast<float>(cval)) == cval;
+  const bool use_f32 = f32_in && fill_exact;
+  const size_t fsz = use_f32 ? sizeof(float) : sizeof(double);
   const long long L = a.L;
-  const size_t row_smem = sizeof(double) * ((size_t)kRowSeg + size - 1);
-  const size_t col_smem = sizeof(double) * kColTI * ((size_t)kColTL + size - 1);
+  // fold_block reads window elements up to (size rounded up to P) + P - 1
+  // past a thread's first output: the tiles are sized for that
+  const size_t row_span = (size_t)kRowSeg + (size + kRowP - 1) / kRowP * kRowP + kRowP;
+  const size_t col_span = (size_t)kColTL + (size + kColP - 1) / kColP * kColP + kColP;
+  const size_t row_smem = fsz * (row_span + row_span / 4 + 1);
+  const size_t col_smem = fsz * kColTI * col_span;
   if (inner == 1 && row_smem <= (size_t)kMaxSmem) {
     a.tiles_b = (L + kRowSeg - 1) / kRowSeg;
     const long long blocks = outer * a.tiles_b;
     if (blocks <= 0x7fffffffLL) {
-      k_minmax_rows<<<(unsigned)blocks, kRowT, row_smem, st>>>(a);
+      if (use_f32) k_minmax_rows<float><<<(unsigned)blocks, kRowT, row_smem, st>>>(a);
+      else k_minmax_rows<double><<<(unsigned)blocks, kRowT, row_smem, st>>>(a);
       return cuda_fail(cudaGetLastError(), "min/max filter launch");
     }
   } else if (inner > 1 && col_smem <= (size_t)kMaxSmem) {
@@ -174,7 +231,8 @@ extern "C" int cimx_min_max_1d(const CimxArray* in, const CimxArray* out, int si
     a.tiles_b = (L + kColTL - 1) / kColTL;
     const long long blocks = a.tiles_a * a.tiles_b * outer;
     if (blocks <= 0x7fffffffLL) {
-      k_minmax_cols<<<(unsigned)blocks, dim3(kColTI, kColTY), col_smem, st>>>(a);
+      if (use_f32) k_minmax_cols<float><<<(unsigned)blocks, dim3(kColTI, kColTY), col_smem, st>>>(a);
+      else k_minmax_cols<double><<<(unsigned)blocks, dim3(kColTI, kColTY), col_smem, st>>>(a);
       return cuda_fail(cudaGetLastError(), "min/max filter launch");
     }
   }

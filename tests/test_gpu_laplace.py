@@ -217,3 +217,22 @@ def test_min_max_filter1d_tiles(ndi, dtype, mode):
                     np.testing.assert_array_equal(got.view(u)[~nan], exp.view(u)[~nan])
                 else:
                     np.testing.assert_array_equal(got, exp)
+
+
+@pytest.mark.parametrize("dtype,cval", [(np.float32, 0.1), (np.float32, 2.5), (np.float16, 0.1),
+                                        (np.float16, -7.0), (np.int32, 3.0)])
+def test_min_max_filter1d_fold_precision(ndi, dtype, cval):
+    """The fold runs in float32 when every value it sees is exact there
+    (8/16-bit and float16/float32 inputs, a fill value float32 holds) and in
+    float64 otherwise (a fill value like 0.1, 32-bit integer inputs); both
+    give the reference's float64 fold."""
+    x = _data((40, 1100), dtype)
+    xd = dev(x)
+    for axis in (0, 1):
+        for name in ("minimum_filter1d", "maximum_filter1d"):
+            for output in (None, np.float64):
+                got = host(getattr(ndi, name)(xd, 7, axis, mode="constant", cval=cval,
+                                              output=output))
+                exp = getattr(R, name)(x, 7, axis, mode="constant", cval=cval, output=output)
+                assert got.dtype == exp.dtype
+                np.testing.assert_array_equal(got, exp)
