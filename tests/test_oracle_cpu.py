@@ -360,3 +360,18 @@ def test_min_max_filter1d_matches_scipy(mode):
     xi = np.random.default_rng(7).integers(0, 255, (30, 50)).astype(np.uint8)
     np.testing.assert_array_equal(R.maximum_filter1d(xi, 5, 0, mode=mode, cval=17),
                                   sndi.maximum_filter1d(xi, 5, 0, mode=mode, cval=17))
+
+
+def test_min_max_fold_is_minimum_number():
+    """The oracle's min / max fold is IEEE 754-2019 minimumNumber /
+    maximumNumber (CUDA's fmin / fmax on the GPU): nan ignored unless every
+    value is nan, and -0 below +0 in either order. Windows of two along a
+    length-2 axis, so both operand orders occur."""
+    pz, nz, nan = 0.0, -0.0, np.nan
+    x = np.array([[pz, nz], [nz, pz], [nan, 1.0], [1.0, nan], [nan, nan]], np.float64)
+    mn = R.minimum_filter1d(x, 2, axis=1, mode="wrap")
+    mx = R.maximum_filter1d(x, 2, axis=1, mode="wrap")
+    assert np.all(np.signbit(mn[:2])) and not np.any(np.signbit(mx[:2]))
+    assert np.array_equal(mn[2:4], [[1.0, 1.0], [1.0, 1.0]])
+    assert np.array_equal(mx[2:4], [[1.0, 1.0], [1.0, 1.0]])
+    assert np.all(np.isnan(mn[4])) and np.all(np.isnan(mx[4]))
