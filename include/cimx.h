@@ -277,7 +277,9 @@ CIMX_API int cimx_any_negative(const CimxArray* a, int* result, void* stream);
  * elements along `axis` (_vendored/_ndimage_filters.py:1362-1497): the
  * element itself, then the window in order, folded with fmin / fmax in
  * double (nan-ignoring); cval (as a double) outside the array in constant
- * mode; cast<D>() on store. C-contiguous arrays of any real dtype. */
+ * mode; cast<D>() on store. C-contiguous arrays of any real dtype. The fold
+ * runs in float32 where every value it sees is exact there (inputs of at
+ * most float32 precision, a cval float32 holds): the same results. */
 CIMX_API int cimx_min_max_1d(const CimxArray* in, const CimxArray* out, int size, int axis,
                              int origin, int mode, double cval, int is_max, void* stream);
 
