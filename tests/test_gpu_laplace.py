@@ -236,3 +236,22 @@ def test_min_max_filter1d_fold_precision(ndi, dtype, cval):
                 exp = getattr(R, name)(x, 7, axis, mode="constant", cval=cval, output=output)
                 assert got.dtype == exp.dtype
                 np.testing.assert_array_equal(got, exp)
+
+
+@pytest.mark.parametrize("mode", ["reflect", "mirror", "nearest", "wrap", "constant"])
+@pytest.mark.parametrize("shape,axes", [((9, 70, 300), None), ((9, 70, 300), (2, 0)),
+                                        ((40, 1000), None), ((40, 1000), (1,)), ((777,), None)])
+def test_laplace_modes_axes_in_place(ndi, mode, shape, axes):
+    """float32 laplace over every mode, axis subsets and orders, 1-D to 3-D,
+    signed zeros: bit for bit the oracle (one pass per axis into the output
+    and a temporary, added in place), also with the output overlapping the
+    input."""
+    x = _data(shape, np.float32)
+    x.flat[::97] = -0.0
+    xd = dev(x)
+    got = host(ndi.laplace(xd, mode=mode, cval=1.25, axes=axes))
+    exp = R.laplace(x, mode=mode, cval=1.25, axes=axes)
+    np.testing.assert_array_equal(got.view(np.uint32), exp.view(np.uint32))
+    y = xd.clone()
+    ndi.laplace(y, output=y, mode=mode, cval=1.25, axes=axes)
+    np.testing.assert_array_equal(host(y).view(np.uint32), exp.view(np.uint32))
